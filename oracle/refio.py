@@ -1,0 +1,82 @@
+"""Test infrastructure: talk to the compiled reference harness (oracle/_ref/).
+
+``write_case`` writes a :class:`adh_kraken_b200.mesh.SW2Case` in the harness's
+binary case format (read by ``read_case`` in oracle/ref_harness.c);
+``read_records`` parses the harness's output; ``run_harness`` runs one mode.
+Only tests, the smoke check, fixture generation and bench.py's CPU-baseline leg use
+this module.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HARNESS = os.path.join(HERE, "_ref", "adh_ref_harness")
+
+
+def harness_available() -> bool:
+    return os.path.exists(HARNESS)
+
+
+def write_case(case, path, sol=None, sol_old=None, sol_older=None):
+    V = case.nnodes
+    sol0 = case.sol0 if sol is None else sol
+    so = case.sol0 if sol_old is None else sol_old
+    soo = case.sol0 if sol_older is None else sol_older
+    with open(path, "wb") as f:
+        f.write(struct.pack("<ii", 0x43325753, 1))
+        f.write(struct.pack("<5i", V, case.ntri, case.nseg, case.nsteps, case.max_nonlin_it))
+        f.write(struct.pack("<5d", case.dt, case.t0, case.tol_nonlin, case.inc_nonlin, case.gravity))
+        f.write(np.ascontiguousarray(case.xyz, dtype="<f8").tobytes())
+        f.write(np.ascontiguousarray(case.tri, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(case.seg, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(case.seg_kind, dtype="<i4").tobytes())
+        for a in (sol0, so, soo):
+            f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+        f.write(struct.pack("<i", len(case.series)))
+        for sid in sorted(case.series):
+            t, v = case.series[sid]
+            f.write(struct.pack("<ii", sid, len(t)))
+            f.write(np.ascontiguousarray(t, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
+
+
+def read_records(path):
+    out = {}
+    with open(path, "rb") as f:
+        data = f.read()
+    pos = 0
+    while pos < len(data):
+        name = data[pos:pos + 32].split(b"\0", 1)[0].decode()
+        typ = chr(data[pos + 32])
+        (count,) = struct.unpack_from("<q", data, pos + 33)
+        pos += 41
+        dt = np.dtype("<f8") if typ == "d" else np.dtype("<i4")
+        out[name] = np.frombuffer(data, dtype=dt, count=count, offset=pos).copy()
+        pos += count * dt.itemsize
+    return out
+
+
+def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=None, env=None, timeout=3600):
+    if not harness_available():
+        raise RuntimeError("reference harness not built (oracle/_ref/adh_ref_harness)")
+    with tempfile.TemporaryDirectory() as td:
+        cpath = os.path.join(td, "case.bin")
+        opath = os.path.join(td, "out.bin")
+        if case is not None:
+            write_case(case, cpath, sol, sol_old, sol_older)
+        else:
+            cpath = "-"
+        e = dict(os.environ)
+        if env:
+            e.update(env)
+        r = subprocess.run([HARNESS, mode, cpath, opath, *map(str, extra)], capture_output=True, env=e,
+                           timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"harness {mode} failed ({r.returncode}): {r.stderr.decode()[-2000:]}")
+        return read_records(opath)
