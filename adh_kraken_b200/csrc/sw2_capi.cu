@@ -1,0 +1,794 @@
+// C ABI and host driver of the B200 SW2 time step (declared in include/adh_sw2_gpu.h).
+//
+// The driver mirrors fe_newton (src/newton/fe_newton.c:44-915) and advance_time
+// (src/timeloop/time_loop.c:56-89) step for step, but every array lives in HBM:
+// the host only reads back the handful of scalars that steer the Newton loop
+// (residual norms, the BiCGStab stop flag).  BiCGStab iterations are replayed
+// from a captured CUDA graph in chunks, with the stop test evaluated on the
+// device, so a converged solve wastes at most one chunk of early-exit launches.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include <string>
+#include "../../include/adh_sw2_gpu.h"
+#include "sw2_launch.h"
+
+using namespace sw2;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+extern "C" const char* sw2g_last_error(void) { return g_err.c_str(); }
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            g_err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+            return SW2G_ERR_CUDA;                                                            \
+        }                                                                                    \
+    } while (0)
+#define CKL()                                                                                \
+    do {                                                                                     \
+        cudaError_t e_ = cudaGetLastError();                                                 \
+        if (e_ != cudaSuccess) {                                                             \
+            g_err = std::string("kernel launch: ") + cudaGetErrorString(e_);                 \
+            return SW2G_ERR_CUDA;                                                            \
+        }                                                                                    \
+    } while (0)
+#define TRY(x) do { int r_ = (x); if (r_ != SW2G_OK) return r_; } while (0)
+
+static const int kChunk = 8;   // BiCGStab iterations per graph replay
+
+struct ProfRec { int cls; cudaEvent_t a, b; };
+
+struct sw2g_model {
+    int V = 0, T = 0, S = 0, Etot = 0, n = 0, nnz = 0, nslots = 0;
+    cudaStream_t st = nullptr; bool own_stream = false;
+    std::vector<int> h_indptr, h_cols;
+    std::vector<void*> allocs;
+    // mesh
+    int *d_tri = nullptr, *d_seg = nullptr, *d_skind = nullptr;
+    double *d_ex = nullptr, *d_ey = nullptr, *d_ez = nullptr, *d_gx = nullptr, *d_gy = nullptr, *d_djac = nullptr;
+    double *d_snx = nullptr, *d_sny = nullptr, *d_sdjac = nullptr;
+    // CSR and node blocks
+    int *d_indptr = nullptr, *d_cols = nullptr, *d_bptr = nullptr, *d_bcol = nullptr, *d_diag = nullptr;
+    // assembly maps
+    int *d_rptr = nullptr, *d_jptr = nullptr, *d_boff = nullptr, *d_blen = nullptr;
+    uint32_t *d_rmap = nullptr, *d_jmap = nullptr;
+    // resident state
+    double *d_sol = nullptr, *d_sol_old = nullptr, *d_sol_older = nullptr, *d_dirichlet = nullptr, *d_guess = nullptr;
+    int *d_bc_mask = nullptr;
+    bool guess_set = false;
+    // work
+    int *d_wd = nullptr, *d_node_tmp = nullptr;
+    double *d_ER = nullptr, *d_EJ = nullptr, *d_res = nullptr, *d_vals = nullptr, *d_dsol = nullptr;
+    double *d_scale = nullptr, *d_inv = nullptr, *d_x0 = nullptr, *d_b64 = nullptr, *d_t64 = nullptr;
+    double *k_r = nullptr, *k_p = nullptr, *k_Ap = nullptr, *k_q = nullptr, *k_s = nullptr, *k_As = nullptr;
+    float *f_vals = nullptr, *f_inv = nullptr, *f_x = nullptr, *f_r = nullptr, *f_p = nullptr, *f_Ap = nullptr;
+    float *f_q = nullptr, *f_s = nullptr, *f_As = nullptr, *f_b = nullptr;
+    // reductions / scalars
+    double *d_partial = nullptr, *d_rout = nullptr; unsigned int* d_counter = nullptr;
+    KrylovScalars* d_ks = nullptr;
+    double* h_rout = nullptr; KrylovScalars* h_ks = nullptr;
+    cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+    StepParams P{};
+    MeshView M{}; AssemblyMaps A{}; BlockCSR B{};
+    // profiling
+    bool prof = false;
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    double prof_ms[SW2G_NCLASSES] = {0};
+    long long prof_launch[SW2G_NCLASSES] = {0};
+};
+
+template <class T>
+static int dalloc(sw2g_model* m, T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) { g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e); *p = nullptr; return SW2G_ERR_NOMEM; }
+    m->allocs.push_back((void*)*p);
+    return SW2G_OK;
+}
+template <class T>
+static int upload(sw2g_model* m, T** p, const T* h, size_t count) {
+    TRY(dalloc(m, p, count));
+    if (count) CK(cudaMemcpyAsync(*p, h, sizeof(T) * count, cudaMemcpyHostToDevice, m->st));
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ profiling
+static cudaEvent_t ev_get(sw2g_model* m) {
+    if (!m->ev_pool.empty()) { cudaEvent_t e = m->ev_pool.back(); m->ev_pool.pop_back(); return e; }
+    cudaEvent_t e; cudaEventCreate(&e); return e;
+}
+struct ProfScope {
+    sw2g_model* m; int cls; cudaEvent_t a = nullptr;
+    ProfScope(sw2g_model* m_, int c, int launches) : m(m_), cls(c) {
+        m->prof_launch[c] += launches;
+        if (m->prof) { a = ev_get(m); cudaEventRecord(a, m->st); }
+    }
+    ~ProfScope() {
+        if (m->prof) { cudaEvent_t b = ev_get(m); cudaEventRecord(b, m->st); m->prof_pending.push_back({cls, a, b}); }
+    }
+};
+static void prof_collect(sw2g_model* m) {
+    if (m->prof_pending.empty()) return;
+    cudaStreamSynchronize(m->st);
+    for (auto& r : m->prof_pending) {
+        float ms = 0; cudaEventElapsedTime(&ms, r.a, r.b);
+        m->prof_ms[r.cls] += ms;
+        m->ev_pool.push_back(r.a); m->ev_pool.push_back(r.b);
+    }
+    m->prof_pending.clear();
+}
+
+// ------------------------------------------------------------------ setup helpers
+// Serial CSR of slin_sys_init_sparsity_mono (slin_sys_init_sparsity_mono.c:335-436)
+// for an all-SW2 mesh: row 3a+v lists 3b+w for every node b sharing an element with
+// a (a itself included), sorted.
+static void build_csr(int V, int T, int S, const int* tri, const int* seg, std::vector<int>& indptr,
+                      std::vector<int>& cols) {
+    std::vector<int> cnt(V + 1, 0);
+    for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) cnt[tri[3 * e + a]] += 3;
+    for (int e = 0; e < S; e++) for (int a = 0; a < 2; a++) cnt[seg[2 * e + a]] += 2;
+    std::vector<long> ptr(V + 1, 0);
+    for (int i = 0; i < V; i++) ptr[i + 1] = ptr[i] + cnt[i];
+    std::vector<int> buf(ptr[V]);
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) { int i = tri[3 * e + a]; for (int b = 0; b < 3; b++) buf[ptr[i] + cnt[i]++] = tri[3 * e + b]; }
+    for (int e = 0; e < S; e++) for (int a = 0; a < 2; a++) { int i = seg[2 * e + a]; for (int b = 0; b < 2; b++) buf[ptr[i] + cnt[i]++] = seg[2 * e + b]; }
+    indptr.assign(3 * (size_t)V + 1, 0);
+    cols.clear();
+    cols.reserve((size_t)ptr[V] * 3);
+    std::vector<int> uniq;
+    for (int i = 0; i < V; i++) {
+        uniq.assign(buf.begin() + ptr[i], buf.begin() + ptr[i + 1]);
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        for (int v = 0; v < 3; v++) {
+            for (int b : uniq) for (int w = 0; w < 3; w++) cols.push_back(3 * b + w);
+            indptr[3 * i + v + 1] = (int)cols.size();
+        }
+    }
+}
+
+extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
+    o->tol_nonlin = 1e-8; o->inc_nonlin = 1e-6; o->max_nonlin_it = 10; o->max_linesearch_cuts = 5;
+    o->krylov_max_it = 4000; o->krylov_tol = 1e-11; o->krylov_precision = 64;
+    o->refine_tol = 1e-6; o->max_refine = 6; o->use_guess = 0;
+}
+
+extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
+    if (!mesh || !out || mesh->nnodes <= 0 || mesh->ntri <= 0 || mesh->nseg < 0 || !mesh->xyz || !mesh->tri ||
+        (mesh->nseg > 0 && (!mesh->seg || !mesh->seg_kind))) {
+        g_err = "sw2g_create: bad mesh description";
+        return SW2G_ERR_ARG;
+    }
+    const int V = mesh->nnodes, T = mesh->ntri, S = mesh->nseg;
+    if ((long)(T + S) * 9 >= (1L << 31) || 3L * V >= (1L << 31)) { g_err = "sw2g_create: mesh too large for 32-bit maps"; return SW2G_ERR_ARG; }
+    for (long i = 0; i < 3L * T; i++) if (mesh->tri[i] < 0 || mesh->tri[i] >= V) { g_err = "sw2g_create: triangle node id out of range"; return SW2G_ERR_MESH; }
+    for (long i = 0; i < 2L * S; i++) if (mesh->seg[i] < 0 || mesh->seg[i] >= V) { g_err = "sw2g_create: segment node id out of range"; return SW2G_ERR_MESH; }
+    sw2g_model* m = new sw2g_model();
+    m->V = V; m->T = T; m->S = S; m->Etot = T + S; m->n = 3 * V;
+    if (cuda_stream) m->st = (cudaStream_t)cuda_stream;
+    else {
+        cudaError_t e = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { g_err = std::string("cudaStreamCreate: ") + cudaGetErrorString(e); delete m; return SW2G_ERR_CUDA; }
+        m->own_stream = true;
+    }
+    int rc = SW2G_OK;
+    auto fail = [&](int r) { sw2g_destroy(m); return r; };
+
+    // --- geometry: selem2d_get_triangle_linear_djac_nrml_gradPhi (src/structs/selem/selem_2d.c:270-350)
+    //     and selem1d_load (src/structs/selem/selem_1d.c:27-58), evaluated in that order of operations
+    std::vector<double> ex(3 * (size_t)T), ey(3 * (size_t)T), ez(3 * (size_t)T), gx(3 * (size_t)T), gy(3 * (size_t)T), dj(T);
+    for (int e = 0; e < T; e++) {
+        const double* p[3];
+        for (int a = 0; a < 3; a++) p[a] = mesh->xyz + 3 * (size_t)mesh->tri[3 * e + a];
+        double s1x = p[1][0] - p[0][0], s1y = p[1][1] - p[0][1];
+        double s2x = p[2][0] - p[0][0], s2y = p[2][1] - p[0][1];
+        double djac = (s1x * s2y) - (s2x * s1y);
+        if (!(fabs(djac) > 2.220446049250313080847e-16)) { g_err = "sw2g_create: degenerate triangle"; return fail(SW2G_ERR_MESH); }
+        double inv = 1. / djac;
+        double g[6] = {(s1y - s2y) * inv, (s2x - s1x) * inv, s2y * inv, -s2x * inv, -s1y * inv, s1x * inv};
+        for (int a = 0; a < 3; a++) {
+            ex[(size_t)a * T + e] = p[a][0]; ey[(size_t)a * T + e] = p[a][1]; ez[(size_t)a * T + e] = p[a][2];
+            gx[(size_t)a * T + e] = g[2 * a]; gy[(size_t)a * T + e] = g[2 * a + 1];
+        }
+        dj[e] = djac * (1.0 / 2.0);
+        if (!(dj[e] > 1e-6)) { g_err = "sw2g_create: triangle not counter-clockwise (selem2d_load rejects it)"; return fail(SW2G_ERR_MESH); }
+    }
+    std::vector<double> snx(S + 1), sny(S + 1), sdj(S + 1);
+    for (int k = 0; k < S; k++) {
+        const double* a = mesh->xyz + 3 * (size_t)mesh->seg[2 * k];
+        const double* b = mesh->xyz + 3 * (size_t)mesh->seg[2 * k + 1];
+        double d = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]));
+        if (!(d > 1e-6)) { g_err = "sw2g_create: zero-length boundary segment"; return fail(SW2G_ERR_MESH); }
+        sdj[k] = d; snx[k] = (b[1] - a[1]) / d; sny[k] = -(b[0] - a[0]) / d;
+    }
+
+    // --- CSR (bit-exact with the reference) and its node-block view
+    build_csr(V, T, S, mesh->tri, S ? mesh->seg : nullptr, m->h_indptr, m->h_cols);
+    const std::vector<int>& ip = m->h_indptr; const std::vector<int>& cl = m->h_cols;
+    m->nnz = (int)cl.size();
+    if (mesh->indptr && mesh->cols) {
+        for (int i = 0; i <= m->n; i++) if (mesh->indptr[i] != ip[i]) { g_err = "sw2g_create: caller CSR row pointers differ from the reference sparsity"; return fail(SW2G_ERR_MESH); }
+        for (int k = 0; k < m->nnz; k++) if (mesh->cols[k] != cl[k]) { g_err = "sw2g_create: caller CSR columns differ from the reference sparsity"; return fail(SW2G_ERR_MESH); }
+    }
+    std::vector<int> bptr(V + 1, 0), bcol, diag(m->n);
+    for (int a = 0; a < V; a++) {
+        int len = ip[3 * a + 1] - ip[3 * a];
+        bptr[a + 1] = bptr[a] + len / 3;
+        for (int j = 0; j < len / 3; j++) bcol.push_back(cl[ip[3 * a] + 3 * j] / 3);
+    }
+    m->nslots = bptr[V];
+    for (int r = 0; r < m->n; r++) {
+        int a = r / 3, j = (int)(std::lower_bound(bcol.begin() + bptr[a], bcol.begin() + bptr[a + 1], a) - bcol.begin()) - bptr[a];
+        diag[r] = ip[r] + 3 * j + r % 3;
+    }
+
+    // --- deterministic assembly maps, in element order (triangles, then segments)
+    std::vector<int> rptr(V + 1, 0);
+    for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) rptr[mesh->tri[3 * e + a] + 1]++;
+    for (int s = 0; s < S; s++) for (int a = 0; a < 2; a++) rptr[mesh->seg[2 * s + a] + 1]++;
+    for (int i = 0; i < V; i++) rptr[i + 1] += rptr[i];
+    std::vector<uint32_t> rmap(rptr[V]);
+    {
+        std::vector<int> fill(rptr.begin(), rptr.end() - 1);
+        for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) rmap[fill[mesh->tri[3 * e + a]]++] = (uint32_t)(3 * e + a);
+        for (int s = 0; s < S; s++) for (int a = 0; a < 2; a++) rmap[fill[mesh->seg[2 * s + a]]++] = (uint32_t)(3 * (T + s) + a);
+    }
+    auto slot = [&](int a, int b) -> int {
+        auto it = std::lower_bound(bcol.begin() + bptr[a], bcol.begin() + bptr[a + 1], b);
+        return (int)(it - bcol.begin());
+    };
+    std::vector<int> jptr(m->nslots + 1, 0);
+    std::vector<int> eslot(9 * (size_t)T + 4 * (size_t)S);
+    for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) {
+        int k = slot(mesh->tri[3 * e + a], mesh->tri[3 * e + b]);
+        eslot[9 * (size_t)e + 3 * a + b] = k; jptr[k + 1]++;
+    }
+    for (int s = 0; s < S; s++) for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) {
+        int k = slot(mesh->seg[2 * s + a], mesh->seg[2 * s + b]);
+        eslot[9 * (size_t)T + 4 * (size_t)s + 2 * a + b] = k; jptr[k + 1]++;
+    }
+    for (int k = 0; k < m->nslots; k++) jptr[k + 1] += jptr[k];
+    std::vector<uint32_t> jmap(jptr[m->nslots]);
+    {
+        std::vector<int> fill(jptr.begin(), jptr.end() - 1);
+        for (int e = 0; e < T; e++) for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++)
+            jmap[fill[eslot[9 * (size_t)e + 3 * a + b]]++] = (uint32_t)(9 * e + 3 * a + b);
+        for (int s = 0; s < S; s++) for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++)
+            jmap[fill[eslot[9 * (size_t)T + 4 * (size_t)s + 2 * a + b]]++] = (uint32_t)(9 * (T + s) + 3 * a + b);
+    }
+    std::vector<int> boff(m->nslots), blen(m->nslots);
+    for (int a = 0; a < V; a++) for (int k = bptr[a]; k < bptr[a + 1]; k++) {
+        boff[k] = ip[3 * a] + 3 * (k - bptr[a]);
+        blen[k] = ip[3 * a + 1] - ip[3 * a];
+    }
+
+    // --- device copies
+    if ((rc = upload(m, &m->d_tri, mesh->tri, 3 * (size_t)T))) return fail(rc);
+    std::vector<int> segv(2 * (size_t)S + 2, 0), kindv(S + 1, 0);
+    for (long i = 0; i < 2L * S; i++) segv[i] = mesh->seg[i];
+    for (int i = 0; i < S; i++) kindv[i] = mesh->seg_kind[i];
+    if ((rc = upload(m, &m->d_seg, segv.data(), segv.size()))) return fail(rc);
+    if ((rc = upload(m, &m->d_skind, kindv.data(), kindv.size()))) return fail(rc);
+    if ((rc = upload(m, &m->d_ex, ex.data(), ex.size())) || (rc = upload(m, &m->d_ey, ey.data(), ey.size())) ||
+        (rc = upload(m, &m->d_ez, ez.data(), ez.size())) || (rc = upload(m, &m->d_gx, gx.data(), gx.size())) ||
+        (rc = upload(m, &m->d_gy, gy.data(), gy.size())) || (rc = upload(m, &m->d_djac, dj.data(), dj.size())) ||
+        (rc = upload(m, &m->d_snx, snx.data(), snx.size())) || (rc = upload(m, &m->d_sny, sny.data(), sny.size())) ||
+        (rc = upload(m, &m->d_sdjac, sdj.data(), sdj.size())))
+        return fail(rc);
+    if ((rc = upload(m, &m->d_indptr, ip.data(), ip.size())) || (rc = upload(m, &m->d_cols, cl.data(), cl.size())) ||
+        (rc = upload(m, &m->d_bptr, bptr.data(), bptr.size())) || (rc = upload(m, &m->d_bcol, bcol.data(), bcol.size())) ||
+        (rc = upload(m, &m->d_diag, diag.data(), diag.size())) || (rc = upload(m, &m->d_rptr, rptr.data(), rptr.size())) ||
+        (rc = upload(m, &m->d_rmap, rmap.data(), rmap.size())) || (rc = upload(m, &m->d_jptr, jptr.data(), jptr.size())) ||
+        (rc = upload(m, &m->d_jmap, jmap.data(), jmap.size())) || (rc = upload(m, &m->d_boff, boff.data(), boff.size())) ||
+        (rc = upload(m, &m->d_blen, blen.data(), blen.size())))
+        return fail(rc);
+    const size_t n = m->n;
+    if ((rc = dalloc(m, &m->d_sol, n)) || (rc = dalloc(m, &m->d_sol_old, n)) || (rc = dalloc(m, &m->d_sol_older, n)) ||
+        (rc = dalloc(m, &m->d_dirichlet, n)) || (rc = dalloc(m, &m->d_guess, n)) || (rc = dalloc(m, &m->d_bc_mask, n)) ||
+        (rc = dalloc(m, &m->d_wd, T)) || (rc = dalloc(m, &m->d_node_tmp, V)) ||
+        (rc = dalloc(m, &m->d_ER, 9 * (size_t)m->Etot)) || (rc = dalloc(m, &m->d_EJ, 81 * (size_t)m->Etot)) ||
+        (rc = dalloc(m, &m->d_res, n)) || (rc = dalloc(m, &m->d_vals, (size_t)m->nnz)) || (rc = dalloc(m, &m->d_dsol, n)) ||
+        (rc = dalloc(m, &m->d_scale, n)) || (rc = dalloc(m, &m->d_inv, 9 * (size_t)V)) || (rc = dalloc(m, &m->d_x0, n)) ||
+        (rc = dalloc(m, &m->d_b64, n)) || (rc = dalloc(m, &m->d_t64, n)) ||
+        (rc = dalloc(m, &m->k_r, n)) || (rc = dalloc(m, &m->k_p, n)) || (rc = dalloc(m, &m->k_Ap, n)) ||
+        (rc = dalloc(m, &m->k_q, n)) || (rc = dalloc(m, &m->k_s, n)) || (rc = dalloc(m, &m->k_As, n)) ||
+        (rc = dalloc(m, &m->d_partial, 4 * (size_t)kMaxBlocks)) || (rc = dalloc(m, &m->d_rout, 8)) ||
+        (rc = dalloc(m, &m->d_counter, 1)) || (rc = dalloc(m, &m->d_ks, 1)))
+        return fail(rc);
+    CK(cudaMemsetAsync(m->d_counter, 0, sizeof(unsigned int), m->st));
+    CK(cudaMemsetAsync(m->d_bc_mask, 0, sizeof(int) * n, m->st));
+    CK(cudaMemsetAsync(m->d_dirichlet, 0, sizeof(double) * n, m->st));
+    CK(cudaMemsetAsync(m->d_EJ, 0, sizeof(double) * 81 * (size_t)m->Etot, m->st));
+    CK(cudaMemsetAsync(m->d_ER, 0, sizeof(double) * 9 * (size_t)m->Etot, m->st));
+    if (cudaMallocHost((void**)&m->h_rout, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost((void**)&m->h_ks, sizeof(KrylovScalars)) != cudaSuccess) {
+        g_err = "cudaMallocHost failed"; return fail(SW2G_ERR_NOMEM);
+    }
+    m->M = MeshView{V, T, S, m->d_tri, m->d_ex, m->d_ey, m->d_ez, m->d_gx, m->d_gy, m->d_djac,
+                    m->d_seg, m->d_snx, m->d_sny, m->d_sdjac, m->d_skind};
+    m->A = AssemblyMaps{m->nslots, m->d_rptr, m->d_rmap, m->d_jptr, m->d_jmap, m->d_boff, m->d_blen};
+    m->B = BlockCSR{V, m->n, m->nnz, m->d_indptr, m->d_cols, m->d_bptr, m->d_bcol, m->d_diag};
+    m->P = StepParams{1.0, 0.0, mesh->gravity, 0.0, 0.0, 0.0};
+    CK(cudaStreamSynchronize(m->st));
+    *out = m;
+    return SW2G_OK;
+}
+
+static int alloc_fp32(sw2g_model* m) {
+    if (m->f_vals) return SW2G_OK;
+    const size_t n = m->n;
+    TRY(dalloc(m, &m->f_vals, (size_t)m->nnz)); TRY(dalloc(m, &m->f_inv, 9 * (size_t)m->V));
+    TRY(dalloc(m, &m->f_x, n)); TRY(dalloc(m, &m->f_r, n)); TRY(dalloc(m, &m->f_p, n)); TRY(dalloc(m, &m->f_Ap, n));
+    TRY(dalloc(m, &m->f_q, n)); TRY(dalloc(m, &m->f_s, n)); TRY(dalloc(m, &m->f_As, n)); TRY(dalloc(m, &m->f_b, n));
+    return SW2G_OK;
+}
+
+extern "C" void sw2g_destroy(sw2g_model* m) {
+    if (!m) return;
+    if (m->st) cudaStreamSynchronize(m->st);
+    if (m->graph64) cudaGraphExecDestroy(m->graph64);
+    if (m->graph32) cudaGraphExecDestroy(m->graph32);
+    for (void* p : m->allocs) cudaFree(p);
+    if (m->h_rout) cudaFreeHost(m->h_rout);
+    if (m->h_ks) cudaFreeHost(m->h_ks);
+    for (auto& r : m->prof_pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : m->ev_pool) cudaEventDestroy(e);
+    if (m->own_stream) cudaStreamDestroy(m->st);
+    delete m;
+}
+
+extern "C" int sw2g_sizes(const sw2g_model* m, int* ndofs, int* nnz) {
+    if (!m) { g_err = "null model"; return SW2G_ERR_ARG; }
+    if (ndofs) *ndofs = m->n;
+    if (nnz) *nnz = m->nnz;
+    return SW2G_OK;
+}
+extern "C" int sw2g_get_sparsity(const sw2g_model* m, int* indptr, int* cols) {
+    if (!m || !indptr || !cols) { g_err = "sw2g_get_sparsity: null argument"; return SW2G_ERR_ARG; }
+    memcpy(indptr, m->h_indptr.data(), sizeof(int) * m->h_indptr.size());
+    memcpy(cols, m->h_cols.data(), sizeof(int) * m->h_cols.size());
+    return SW2G_OK;
+}
+extern "C" int sw2g_set_step(sw2g_model* m, double dt, double tau, double bc_depth, double bc_vx, double bc_vy) {
+    if (!m || !(dt > 0)) { g_err = "sw2g_set_step: bad model or dt"; return SW2G_ERR_ARG; }
+    m->P.dt = dt; m->P.alpha = tau; m->P.bc_depth = bc_depth; m->P.bc_vx = bc_vx; m->P.bc_vy = bc_vy;
+    return SW2G_OK;
+}
+extern "C" void* sw2g_stream(sw2g_model* m) { return m ? (void*)m->st : nullptr; }
+extern "C" int sw2g_device_state(sw2g_model* m, double** sol, double** sol_old, double** sol_older) {
+    if (!m) { g_err = "null model"; return SW2G_ERR_ARG; }
+    if (sol) *sol = m->d_sol; if (sol_old) *sol_old = m->d_sol_old; if (sol_older) *sol_older = m->d_sol_older;
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ building blocks
+static int do_wd(sw2g_model* m, const double* sol, const double* sol_old) {
+    ProfScope ps(m, 5, 3);
+    launch_wd_flags(m->M, sol, sol_old, m->d_node_tmp, m->d_wd, m->st);
+    CKL();
+    return SW2G_OK;
+}
+static int do_residual(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older, double* res) {
+    ProfScope ps(m, 0, 3);
+    launch_elem_resid(m->M, m->P, sol, sol_old, sol_older, m->d_wd, m->d_ER, m->st);
+    launch_gather_resid(m->V, m->A, m->d_ER, res, m->st);
+    CKL();
+    return SW2G_OK;
+}
+static int do_jacobian(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older, double* vals) {
+    {
+        ProfScope ps(m, 1, 4);
+        launch_elem_jac(m->M, m->P, sol, sol_old, sol_older, m->d_wd, m->d_EJ, m->st);
+        CKL();
+    }
+    ProfScope ps(m, 2, 1);
+    launch_gather_jac(m->A, m->d_EJ, m->Etot, vals, m->st);
+    CKL();
+    return SW2G_OK;
+}
+static int do_norms(sw2g_model* m, const double* res, const double* dsol, double* rmax, double* rl2, double* imax) {
+    {
+        ProfScope ps(m, 5, 1);
+        Reduce R{m->d_partial, m->d_counter, m->d_rout};
+        launch_norms(m->n, res, dsol, m->d_bc_mask, R, m->st);
+        CKL();
+    }
+    CK(cudaMemcpyAsync(m->h_rout, m->d_rout, 3 * sizeof(double), cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    *rmax = m->h_rout[0]; *rl2 = sqrt(m->h_rout[1]) / m->n; *imax = m->h_rout[2];
+    return SW2G_OK;
+}
+// check_diag + apply_Dirichlet_BC + scale_linear_system on device arrays
+static int do_prepare(sw2g_model* m, double* vals, double* res, double* x) {
+    ProfScope ps(m, 3, 4);
+    launch_check_diag(m->B, vals, m->d_bc_mask, m->st);
+    launch_dirichlet_rowscale(m->B, m->d_bc_mask, vals, res, x, m->d_scale, m->st);
+    launch_scale_vals(m->B, m->d_scale, vals, m->st);
+    launch_bj_setup(m->B, vals, m->d_inv, m->st);
+    CKL();
+    return SW2G_OK;
+}
+
+template <class VT>
+static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, cudaGraphExec_t* graph, int max_it, double atol, double rtol,
+                    int* iters, int* status) {
+    KrylovScalars init{};
+    init.tol = atol; init.rtol = rtol; init.max_it = max_it;
+    Reduce R{m->d_partial, m->d_counter, m->d_rout};
+    {
+        ProfScope ps(m, 4, 2);
+        CK(cudaMemcpyAsync(m->d_ks, &init, sizeof(KrylovScalars), cudaMemcpyHostToDevice, m->st));
+        launch_bicg_init<VT>(m->B, V, m->d_ks, R, m->st);
+        CKL();
+    }
+    if (!*graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+        for (int c = 0; c < kChunk; c++) launch_bicg_iteration<VT>(m->B, V, m->d_ks, R, m->st);
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            g_err = std::string("graph capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2);
+            return SW2G_ERR_CUDA;
+        }
+        CK(cudaGraphInstantiate(graph, g, 0));
+        cudaGraphDestroy(g);
+    }
+    while (true) {
+        CK(cudaMemcpyAsync(m->h_ks, m->d_ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        if (m->h_ks->done) break;
+        ProfScope ps(m, 4, 4 * kChunk);
+        CK(cudaGraphLaunch(*graph, m->st));
+    }
+    *iters = m->h_ks->it;
+    *status = m->h_ks->status;
+    return SW2G_OK;
+}
+
+// Left-preconditioned BiCGStab of bcgstab_solver.c:65-330 on the prepared (scaled)
+// system in d_vals: x (= dsol) in/out with the reference's x0 shift and unscaling;
+// b is overwritten with M^-1 b as in the reference.
+static int solve64(sw2g_model* m, double* x, double* b, int max_it, double tol, int* iters, int* status) {
+    CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * m->n, cudaMemcpyDeviceToDevice, m->st));
+    KrylovVecs<double> V{x, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, b, m->d_vals, m->d_inv};
+    TRY(run_bicg<double>(m, V, &m->graph64, max_it, tol, tol, iters, status));
+    ProfScope ps(m, 5, 1);
+    launch_unscale(m->n, m->d_x0, m->d_scale, x, m->st);
+    CKL();
+    return SW2G_OK;
+}
+
+// FP32 BiCGStab inside FP64 iterative refinement, on the same scaled,
+// block-Jacobi-preconditioned system.  x accumulates in FP64.  Each pass forms the
+// FP64 residual t = b - A x, stops when the reference's test holds for it
+// (max|M^-1 t| <= tol + tol * max|M^-1 b|), and otherwise solves A d = t in FP32
+// to a relative reduction of refine_tol and adds d to x in FP64.
+static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& o, int* iters, int* passes, int* status) {
+    TRY(alloc_fp32(m));
+    const int n = m->n;
+    Reduce R{m->d_partial, m->d_counter, m->d_rout};
+    CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_b64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemsetAsync(x, 0, sizeof(double) * n, m->st));
+    {
+        ProfScope ps(m, 3, 2);
+        launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
+        launch_to_float(9 * m->V, m->d_inv, m->f_inv, m->st);
+        CKL();
+    }
+    *iters = 0; *passes = 0; *status = 0;
+    double bnorm = -1;
+    for (int pass = 0; pass <= o.max_refine; pass++) {
+        {
+            ProfScope ps(m, 4, 1);
+            launch_resid_pnorm(m->B, m->d_vals, m->d_inv, x, m->d_b64, m->d_t64, R, m->st);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        const double rn = m->h_rout[0];
+        if (bnorm < 0) bnorm = rn;                 // x = 0 on the first pass: M^-1 t = M^-1 b
+        if (!std::isfinite(rn)) { *status = 2; break; }
+        if (!(rn > o.krylov_tol + bnorm * o.krylov_tol) || pass == o.max_refine) break;
+        {
+            ProfScope ps(m, 4, 1);
+            launch_to_float(n, m->d_t64, m->f_b, m->st);
+            CKL();
+        }
+        KrylovVecs<float> V32{m->f_x, m->f_r, m->f_p, m->f_Ap, m->f_q, m->f_s, m->f_As, m->f_b, m->f_vals, m->f_inv};
+        int it = 0, st = 0;
+        TRY(run_bicg<float>(m, V32, &m->graph32, o.krylov_max_it, 0.0, o.refine_tol, &it, &st));
+        *iters += it; *passes += 1;
+        if (st == 1 || st == 2) *status = st;
+        {
+            ProfScope ps(m, 5, 2);
+            launch_to_double(n, m->f_x, m->d_t64, m->st);
+            launch_axpy(n, 1.0, m->d_t64, x, m->st);
+            CKL();
+        }
+        if (st == 2) break;
+    }
+    ProfScope ps(m, 5, 1);
+    launch_unscale(n, m->d_x0, m->d_scale, x, m->st);
+    CKL();
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ Newton step
+// fe_newton (src/newton/fe_newton.c:44-915), serial non-PETSc branch, on the
+// resident state d_sol / d_sol_old / d_sol_older / d_bc_mask / d_dirichlet.
+static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_stats* S) {
+    const int n = m->n;
+    sw2g_newton_stats st{};
+    // initialize_system (newton_tools.c:21-53): sol <- sol_old, then fe_sw2_init:
+    // wet/dry flags of (sol, sol_old) and the dry-node velocity masks
+    CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    {
+        ProfScope ps(m, 5, 1);
+        launch_dry_mask(m->V, m->d_sol_old, m->d_bc_mask, m->st);
+        CKL();
+    }
+    // initial-guess hook: after initialize_system, before initialize_dirichlet_bc
+    if (o.use_guess && m->guess_set)
+        CK(cudaMemcpyAsync(m->d_sol, m->d_guess, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    {   // initialize_dirichlet_bc (newton_tools.c:130)
+        ProfScope ps(m, 5, 1);
+        launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
+        CKL();
+    }
+    CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
+    double rmax, rl2, imax;
+    TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+    TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
+    if (!std::isfinite(rl2)) { g_err = "non-finite residual at the initial guess"; return SW2G_ERR_NONFINITE; }
+    st.initial_resid_max = rmax;
+    int it = 0; bool ok = true, keep;
+    do {
+        TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
+        CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
+        TRY(do_prepare(m, m->d_vals, m->d_res, m->d_dsol));
+        int kit = 0, kst = 0, passes = 0;
+        if (o.krylov_precision == 32) TRY(solve32(m, m->d_dsol, m->d_res, o, &kit, &passes, &kst));
+        else TRY(solve64(m, m->d_dsol, m->d_res, o.krylov_max_it, o.krylov_tol, &kit, &kst));
+        st.krylov_its += kit; st.refine_passes += passes;
+        if (kst == 1 || kst == 2) st.krylov_breakdowns++;
+        {   // increment_function (newton_tools.c:261) and dsol = -dsol (fe_newton.c:553-555)
+            ProfScope ps(m, 5, 2);
+            launch_axpy(n, 1.0, m->d_dsol, m->d_sol, m->st);
+            launch_scal(n, -1.0, m->d_dsol, m->st);
+            CKL();
+        }
+        const double old_l2 = rl2;
+        TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+        TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
+        if (std::isnan(rl2) || std::isinf(rl2)) ok = false;
+        int cuts = 0;   // line search, fe_newton.c:681-741
+        while (rmax > o.tol_nonlin && rl2 > old_l2 && cuts < o.max_linesearch_cuts) {
+            {
+                ProfScope ps(m, 5, 2);
+                launch_scal(n, 0.5, m->d_dsol, m->st);
+                launch_axpy(n, 1.0, m->d_dsol, m->d_sol, m->st);
+                CKL();
+            }
+            TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+            TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
+            cuts++;
+        }
+        st.linesearch_cuts += cuts;
+        it++;
+        keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && imax > o.inc_nonlin;
+    } while (keep);
+    st.newton_its = it;
+    st.resid_max = rmax; st.resid_l2 = rl2; st.inc_max = imax;
+    st.success = !((rmax > o.tol_nonlin && imax > o.inc_nonlin) || rmax >= 1.0E+20 || !ok);
+    if (!st.success) {   // fe_newton.c:887-890: reset to the old values
+        CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+        launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
+        CKL();
+    }
+    if (S) *S = st;
+    if (!ok) { g_err = "non-finite residual norm during Newton"; return SW2G_ERR_NONFINITE; }
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+#define NEED(cond, msg) do { if (!(cond)) { g_err = msg; return SW2G_ERR_ARG; } } while (0)
+
+static int put3(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older) {
+    const size_t b = sizeof(double) * m->n;
+    CK(cudaMemcpyAsync(m->d_sol, sol, b, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_sol_old, sol_old, b, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_sol_older, sol_older, b, cudaMemcpyHostToDevice, m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_wd_flags(sw2g_model* m, const double* sol, const double* sol_old, int* wd_flag) {
+    NEED(m && sol && sol_old && wd_flag, "sw2g_wd_flags: null argument");
+    TRY(put3(m, sol, sol_old, sol_old));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    CK(cudaMemcpyAsync(wd_flag, m->d_wd, sizeof(int) * m->T, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_elem_resid(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older,
+                               double* out_tri, double* out_seg) {
+    NEED(m && sol && sol_old && sol_older && out_tri && (m->S == 0 || out_seg), "sw2g_elem_resid: null argument");
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    {
+        ProfScope ps(m, 0, 2);
+        launch_elem_resid(m->M, m->P, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_wd, m->d_ER, m->st);
+        CKL();
+    }
+    std::vector<double> er(9 * (size_t)m->Etot);
+    CK(cudaMemcpyAsync(er.data(), m->d_ER, sizeof(double) * er.size(), cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    memcpy(out_tri, er.data(), sizeof(double) * 9 * (size_t)m->T);
+    for (int s = 0; s < m->S; s++) for (int i = 0; i < 6; i++) out_seg[6 * (size_t)s + i] = er[9 * ((size_t)m->T + s) + i];
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_elem_jac(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older,
+                             double* out_tri, double* out_seg) {
+    NEED(m && sol && sol_old && sol_older && out_tri && (m->S == 0 || out_seg), "sw2g_elem_jac: null argument");
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    {
+        ProfScope ps(m, 1, 4);
+        launch_elem_jac(m->M, m->P, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_wd, m->d_EJ, m->st);
+        CKL();
+    }
+    std::vector<double> ej(81 * (size_t)m->Etot);
+    CK(cudaMemcpyAsync(ej.data(), m->d_EJ, sizeof(double) * ej.size(), cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    const size_t Et = m->Etot;
+    for (size_t e = 0; e < (size_t)m->T; e++)
+        for (int c = 0; c < 9; c++) for (int r = 0; r < 9; r++) out_tri[e * 81 + r * 9 + c] = ej[(c * Et + e) * 9 + r];
+    for (size_t s = 0; s < (size_t)m->S; s++)
+        for (int c = 0; c < 6; c++) for (int r = 0; r < 6; r++) out_seg[s * 36 + r * 6 + c] = ej[(c * Et + m->T + s) * 9 + r];
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_assemble_residual(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older,
+                                      double* residual) {
+    NEED(m && sol && sol_old && sol_older && residual, "sw2g_assemble_residual: null argument");
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+    CK(cudaMemcpyAsync(residual, m->d_res, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_assemble_jacobian(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older,
+                                      double* vals) {
+    NEED(m && sol && sol_old && sol_older && vals, "sw2g_assemble_jacobian: null argument");
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_wd(m, m->d_sol, m->d_sol_old));
+    TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
+    CK(cudaMemcpyAsync(vals, m->d_vals, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_prepare_system(sw2g_model* m, double* vals, double* residual, double* x, int* bc_mask, double* scale) {
+    NEED(m && vals && residual && x && bc_mask && scale, "sw2g_prepare_system: null argument");
+    const size_t n = m->n;
+    CK(cudaMemcpyAsync(m->d_vals, vals, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_res, residual, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_dsol, x, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_bc_mask, bc_mask, sizeof(int) * n, cudaMemcpyHostToDevice, m->st));
+    TRY(do_prepare(m, m->d_vals, m->d_res, m->d_dsol));
+    CK(cudaMemcpyAsync(vals, m->d_vals, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(residual, m->d_res, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(x, m->d_dsol, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(bc_mask, m->d_bc_mask, sizeof(int) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(scale, m->d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_solve_linear_sys_bcgstab(sw2g_model* m, double* x, const double* vals, double* b,
+                                             const double* scale_vect, int max_it, double tol, int* iters) {
+    NEED(m && x && vals && b && scale_vect && max_it >= 0 && tol >= 0, "sw2g_solve_linear_sys_bcgstab: bad argument");
+    const size_t n = m->n;
+    CK(cudaMemcpyAsync(m->d_vals, vals, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_res, b, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_dsol, x, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_scale, scale_vect, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
+    {
+        ProfScope ps(m, 3, 1);
+        launch_bj_setup(m->B, m->d_vals, m->d_inv, m->st);
+        CKL();
+    }
+    int it = 0, status = 0;
+    TRY(solve64(m, m->d_dsol, m->d_res, max_it, tol, &it, &status));
+    CK(cudaMemcpyAsync(x, m->d_dsol, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(b, m->d_res, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    if (iters) *iters = (status == 1 || status == 2) ? -it - 1 : it;
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_load_state(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older,
+                               const int* bc_mask, const double* dirichlet) {
+    NEED(m && sol && sol_old && sol_older, "sw2g_load_state: null argument");
+    TRY(put3(m, sol, sol_old, sol_older));
+    if (bc_mask) CK(cudaMemcpyAsync(m->d_bc_mask, bc_mask, sizeof(int) * m->n, cudaMemcpyHostToDevice, m->st));
+    else CK(cudaMemsetAsync(m->d_bc_mask, 0, sizeof(int) * m->n, m->st));
+    if (dirichlet) CK(cudaMemcpyAsync(m->d_dirichlet, dirichlet, sizeof(double) * m->n, cudaMemcpyHostToDevice, m->st));
+    else CK(cudaMemsetAsync(m->d_dirichlet, 0, sizeof(double) * m->n, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_store_state(sw2g_model* m, double* sol, double* sol_old, double* sol_older, int* bc_mask) {
+    NEED(m, "sw2g_store_state: null model");
+    const size_t b = sizeof(double) * m->n;
+    if (sol) CK(cudaMemcpyAsync(sol, m->d_sol, b, cudaMemcpyDeviceToHost, m->st));
+    if (sol_old) CK(cudaMemcpyAsync(sol_old, m->d_sol_old, b, cudaMemcpyDeviceToHost, m->st));
+    if (sol_older) CK(cudaMemcpyAsync(sol_older, m->d_sol_older, b, cudaMemcpyDeviceToHost, m->st));
+    if (bc_mask) CK(cudaMemcpyAsync(bc_mask, m->d_bc_mask, sizeof(int) * m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_set_guess(sw2g_model* m, const double* guess, int on_device) {
+    NEED(m, "sw2g_set_guess: null model");
+    if (!guess) { m->guess_set = false; return SW2G_OK; }
+    CK(cudaMemcpyAsync(m->d_guess, guess, sizeof(double) * m->n,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, m->st));
+    m->guess_set = true;
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_fe_newton(sw2g_model* m, double* sol, const double* sol_old, const double* sol_older, int* bc_mask,
+                              const double* dirichlet, const sw2g_newton_opts* opts, sw2g_newton_stats* stats) {
+    NEED(m && sol && sol_old && sol_older && bc_mask, "sw2g_fe_newton: null argument");
+    sw2g_newton_opts o; if (opts) o = *opts; else sw2g_default_opts(&o);
+    TRY(sw2g_load_state(m, sol_old, sol_old, sol_older, bc_mask, dirichlet));
+    int rc = newton_device(m, o, stats);
+    CK(cudaMemcpyAsync(sol, m->d_sol, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(bc_mask, m->d_bc_mask, sizeof(int) * m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return rc;
+}
+
+extern "C" int sw2g_step(sw2g_model* m, const sw2g_newton_opts* opts, sw2g_newton_stats* stats) {
+    NEED(m, "sw2g_step: null model");
+    sw2g_newton_opts o; if (opts) o = *opts; else sw2g_default_opts(&o);
+    // smodel_super_prep_sol: sol_older <- sol_old <- sol (a pointer rotation)
+    double* t = m->d_sol_older; m->d_sol_older = m->d_sol_old; m->d_sol_old = m->d_sol; m->d_sol = t;
+    int rc = newton_device(m, o, stats);
+    m->guess_set = false;
+    return rc;
+}
+
+extern "C" int sw2g_set_profiling(sw2g_model* m, int on) {
+    NEED(m, "null model");
+    m->prof = on != 0;
+    return SW2G_OK;
+}
+extern "C" int sw2g_get_profile(sw2g_model* m, double* ms, long long* launches) {
+    NEED(m, "null model");
+    prof_collect(m);
+    for (int c = 0; c < SW2G_NCLASSES; c++) { if (ms) ms[c] = m->prof_ms[c]; if (launches) launches[c] = m->prof_launch[c]; }
+    return SW2G_OK;
+}
+extern "C" int sw2g_reset_profile(sw2g_model* m) {
+    NEED(m, "null model");
+    prof_collect(m);
+    for (int c = 0; c < SW2G_NCLASSES; c++) { m->prof_ms[c] = 0; m->prof_launch[c] = 0; }
+    return SW2G_OK;
+}

@@ -1,0 +1,104 @@
+"""Host-side time loop around the GPU Newton step.
+
+Mirrors the reference's driver layer: time_loop / update_dt / advance_time
+(src/timeloop/time_loop.c:14-125) and the step averaging of the boundary series
+(sseries_setall_ts_valuesAVG, src/structs/sseries/sseries.c:622-682).  The
+per-step work -- residuals, FD Jacobian, assembly, Dirichlet/scaling, BiCGStab,
+Newton -- runs on the device through the C ABI (capi.SW2Model).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .capi import SW2Model, default_opts
+
+_EPS = np.finfo(np.float64).eps
+
+
+def _interval(times, t):
+    # sseries_get_interval (sseries.c:746-773)
+    i = 0
+    n = len(times)
+    while i < n - 1 and t >= times[i] * (1.0 - _EPS):
+        i += 1
+    return i - 1
+
+
+def _eval(times, values, iv, t):
+    # tc_eval_series (src/tools/tc_eval_series.c)
+    if iv == len(times) - 1:
+        return values[-1]
+    lt, rt = times[iv], times[iv + 1]
+    theta = (rt - t) / (rt - lt)
+    return theta * values[iv] + (1.0 - theta) * values[iv + 1]
+
+
+def _trap(lv, rv, lt, rt):
+    # tc_trap_area (src/tools/tc_trap_area.c)
+    d = rt - lt
+    return 0.0 if d < _EPS else (lv + rv) * 0.5 * d
+
+
+def series_step_average(times, values, t1, t2):
+    """Average of a piecewise-linear series over [t1, t2] (sseries_set_values_average)."""
+    times = np.asarray(times, dtype=np.float64)
+    values = np.asarray(values, dtype=np.float64)
+    if t1 < times[0] * (1.0 - _EPS) or t2 > times[-1] * (1.0 + _EPS):
+        raise ValueError(f"time window [{t1}, {t2}] is outside the series range")
+    i1, i2 = _interval(times, t1), _interval(times, t2)
+    v1, v2 = _eval(times, values, i1, t1), _eval(times, values, i2, t2)
+    if i1 == i2:
+        area = _trap(v1, v2, t1, t2)
+    else:
+        area = 0.0
+        for k in range(i1 + 1, i2):
+            area += _trap(values[k], values[k + 1], times[k], times[k + 1])
+        area += _trap(v1, values[i1 + 1], t1, times[i1 + 1])
+        area += _trap(values[i2], v2, times[i2], t2)
+    return area / (t2 - t1)
+
+
+class SW2Simulation:
+    """A time-stepping SW2 run whose state stays resident on the GPU."""
+
+    def __init__(self, case, opts=None, stream=None):
+        self.case = case
+        self.model = SW2Model(case, stream=stream)
+        self.opts = opts or default_opts(tol_nonlin=case.tol_nonlin, inc_nonlin=case.inc_nonlin,
+                                         max_nonlin_it=case.max_nonlin_it)
+        self.t = case.t0
+        sol0 = case.sol0.astype(np.float64)
+        self.model.load_state(sol0, sol0, sol0)
+        self.history = []
+
+    def bc_values(self, t1, t2):
+        s = self.case.series
+        out = [series_step_average(*s[0], t1, t2)]
+        for k in (1, 2):
+            out.append(series_step_average(*s[k], t1, t2) if k in s else 0.0)
+        return out
+
+    def prepare_step(self):
+        """update_dt + the series averaging of advance_time for the next step."""
+        dt = self.case.dt
+        t_new = self.t + dt
+        d, vx, vy = self.bc_values(t_new - dt, t_new)
+        self.model.set_step(dt, d, vx, vy)
+        return t_new
+
+    def step(self, opts=None):
+        t_new = self.prepare_step()
+        st = self.model.step(opts or self.opts)
+        self.t = t_new
+        self.history.append(st)
+        return st
+
+    def run(self, nsteps, opts=None, stop_on_failure=True):
+        for _ in range(nsteps):
+            st = self.step(opts)
+            if stop_on_failure and not st["success"]:
+                break
+        return self.history
+
+    def state(self):
+        return self.model.store_state()

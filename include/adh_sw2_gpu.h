@@ -1,0 +1,150 @@
+/*
+ * adh_sw2_gpu.h -- C ABI of the B200 (sm_100a) implementation of AdH-Kraken's
+ * implicit SW2 time step.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and reports
+ * failures through its int return value (SW2G_OK = 0) and sw2g_last_error().
+ * Host-buffer entry points copy their inputs to the device and their outputs
+ * back, so they drop in where the reference's C routines are called today; the
+ * *_state / sw2g_step entry points keep the solution resident in HBM.
+ *
+ * Conventions are the reference's: node-major dofs (dof = 3*node + {0:h, 1:u, 2:v},
+ * src/structs/sivar_position/sivar_position.c:61-81), the serial CSR of
+ * slin_sys_init_sparsity_mono (sorted unique columns per row), element order =
+ * triangles then boundary segments, and bc_mask entries equal to 1 for Dirichlet
+ * dofs (the reference's YES).
+ *
+ * Not reentrant on one model: calls on a model must come from one host thread,
+ * as in the reference (module-level static work buffers, e.g.
+ * src/la/bcgstab_solver.c:5-22).  Different models are independent.
+ */
+#ifndef ADH_SW2_GPU_H
+#define ADH_SW2_GPU_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SW2G_OK 0
+#define SW2G_ERR_ARG (-1)       /* bad argument or size */
+#define SW2G_ERR_CUDA (-2)      /* CUDA runtime error (message in sw2g_last_error) */
+#define SW2G_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define SW2G_ERR_MESH (-4)      /* mesh / CSR structure not usable */
+#define SW2G_ERR_NONFINITE (-5) /* NaN or Inf in a residual norm (the reference exits, newton_tools.c:344-349) */
+
+typedef struct sw2g_model sw2g_model;
+
+typedef struct {
+    int nnodes, ntri, nseg;
+    const double *xyz;      /* [3*nnodes] x, y, bed elevation z */
+    const int *tri;         /* [3*ntri] counter-clockwise node ids */
+    const int *seg;         /* [2*nseg] boundary segments; node order gives the outward normal */
+    const int *seg_kind;    /* [nseg] 0 = "NB VEL" (fe_sw2_bc_vel), 1 = "DEPTH" (fe_sw2_bc_h) */
+    const int *indptr;      /* optional [3*nnodes+1]: the caller's CSR, checked against ours; NULL to build */
+    const int *cols;        /* optional [nnz] */
+    double gravity;         /* sm->gravity, 9.8 by default */
+} sw2g_mesh;
+
+typedef struct {
+    double tol_nonlin;        /* sm->tol_nonlin, absolute max-norm, default 1e-8 */
+    double inc_nonlin;        /* sm->inc_nonlin, default 1e-6 */
+    int max_nonlin_it;        /* sm->max_nonlin_it, default 10 */
+    int max_linesearch_cuts;  /* sm->max_nonlin_linesearch_cuts, default 5 */
+    int krylov_max_it;        /* BiCGStab iteration cap per solve */
+    double krylov_tol;        /* BiCGStab stopping tolerance (bcgstab_solver.c:20-21: 1e-11) */
+    int krylov_precision;     /* 64: FP64 BiCGStab; 32: FP32 BiCGStab inside FP64 iterative refinement */
+    double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
+    int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
+    int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess instead of sol_old */
+} sw2g_newton_opts;
+
+typedef struct {
+    int newton_its;           /* Newton iterations of the step */
+    int krylov_its;           /* BiCGStab iterations summed over the step */
+    int linesearch_cuts;      /* line-search halvings summed over the step */
+    int refine_passes;        /* FP64 refinement passes (32-bit mode) */
+    int success;              /* fe_newton's TRUE/FALSE */
+    int krylov_breakdowns;    /* BiCGStab solves that stopped on a zero/non-finite denominator */
+    double resid_max;         /* final max |R| over non-Dirichlet dofs */
+    double resid_l2;          /* final sqrt(sum R^2)/ndofs */
+    double inc_max;           /* last max |increment| */
+    double initial_resid_max; /* max |R| at the initial guess */
+} sw2g_newton_stats;
+
+/* --- lifetime ------------------------------------------------------------ */
+/* Builds the device model: element geometry (selem2d/selem1d), the bit-exact CSR
+ * (src/structs/slin_sys/slin_sys_init_sparsity_mono.c:28), the element-to-CSR
+ * assembly maps and all work buffers.  `cuda_stream` may be NULL (own stream).
+ * Replaces the linear-system part of smodel_design_init_no_read
+ * (src/structs/smodel_design/smodel_design_init_no_read.c:110-135). */
+int sw2g_create(const sw2g_mesh *mesh, void *cuda_stream, sw2g_model **out);
+void sw2g_destroy(sw2g_model *m);
+const char *sw2g_last_error(void);
+void sw2g_default_opts(sw2g_newton_opts *opts);
+int sw2g_sizes(const sw2g_model *m, int *ndofs, int *nnz);
+/* The CSR structure the device uses: identical to the reference's serial CSR. */
+int sw2g_get_sparsity(const sw2g_model *m, int *indptr, int *cols);
+/* Per-step scalars: dt = ts->dt / nsubsteps, tau_temporal, and the step-averaged
+ * values of series 0 (depth) and 1/2 (velocity x/y) (sseries_setall_ts_valuesAVG,
+ * src/structs/sseries/sseries.c:673). */
+int sw2g_set_step(sw2g_model *m, double dt, double tau_temporal, double bc_depth, double bc_vx, double bc_vy);
+
+/* --- drop-in host-buffer entry points ------------------------------------ */
+/* fe_sw2_wdflag_legacy (src/models/sw2/sw2_wdflag_legacy.c:34): [ntri] flags 0/1/2 */
+int sw2g_wd_flags(sw2g_model *m, const double *sol, const double *sol_old, int *wd_flag);
+/* Element residuals as the reference's resid plugins return them
+ * (fe_sw2_body_resid sw2_body_resid.c:44, fe_sw2_bc_vel sw2_bc_vel.c:58,
+ * fe_sw2_bc_h sw2_bc_h.c:57): [ntri*9] and [nseg*6].  Uses the wet/dry flags of
+ * (sol, sol_old). */
+int sw2g_elem_resid(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                    double *out_tri, double *out_seg);
+/* Central-difference element Jacobians (perturb_var, src/jacobian/assemble_jacobian.c:304):
+ * [ntri*81] and [nseg*36], row-major element matrices. */
+int sw2g_elem_jac(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                  double *out_tri, double *out_seg);
+/* assemble_residual(SMODEL_SUPER*, SGRID*) (src/residual/residual.h:5): [ndofs] */
+int sw2g_assemble_residual(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                           double *residual);
+/* assemble_jacobian(SMODEL_SUPER*) (src/jacobian/jacobian.h:5): CSR values [nnz] */
+int sw2g_assemble_jacobian(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                           double *vals);
+/* check_diag + apply_Dirichlet_BC (src/la/la.h:12-13) + scale_linear_system (la.h:46):
+ * vals [nnz], residual [ndofs], x [ndofs] and bc_mask [ndofs] in/out; scale [ndofs] out. */
+int sw2g_prepare_system(sw2g_model *m, double *vals, double *residual, double *x, int *bc_mask, double *scale);
+/* solve_linear_sys_bcgstab (src/la/la.h:22-29), serial branch: x in/out (the x0 shift
+ * and the unscaling are the reference's), b is overwritten with M^-1 b as in the
+ * reference.  The exact UMFPACK LU preconditioner is replaced by 3x3 nodal
+ * block-Jacobi.  Returns the iteration count in *iters. */
+int sw2g_solve_linear_sys_bcgstab(sw2g_model *m, double *x, const double *vals, double *b, const double *scale_vect,
+                                  int max_it, double tol, int *iters);
+/* fe_newton(SMODEL_SUPER*) (src/newton/newton.h:19) for one time step: sol out;
+ * sol_old/sol_older in; bc_mask in/out (permanent Dirichlet marks); dirichlet in. */
+int sw2g_fe_newton(sw2g_model *m, double *sol, const double *sol_old, const double *sol_older, int *bc_mask,
+                   const double *dirichlet, const sw2g_newton_opts *opts, sw2g_newton_stats *stats);
+
+/* --- device-resident time stepping --------------------------------------- */
+int sw2g_load_state(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                    const int *bc_mask, const double *dirichlet);
+int sw2g_store_state(sw2g_model *m, double *sol, double *sol_old, double *sol_older, int *bc_mask);
+/* Optional Newton initial guess for the next sw2g_step (host [ndofs] or device pointer). */
+int sw2g_set_guess(sw2g_model *m, const double *guess, int guess_on_device);
+/* One time step on the resident state: smodel_super_prep_sol (sol_older <- sol_old
+ * <- sol) then fe_newton, as advance_time does (src/timeloop/time_loop.c:56-89). */
+int sw2g_step(sw2g_model *m, const sw2g_newton_opts *opts, sw2g_newton_stats *stats);
+/* Device pointers of the resident state (for device-side consumers such as the
+ * learned initial-guess network). */
+int sw2g_device_state(sw2g_model *m, double **sol, double **sol_old, double **sol_older);
+void *sw2g_stream(sw2g_model *m);
+
+/* --- instrumentation ------------------------------------------------------ */
+/* Per kernel class, CUDA-event time (ms) and launch counts since the last reset:
+ * classes 0 residual, 1 FD Jacobian, 2 Jacobian gather, 3 Dirichlet/scale/precond
+ * setup, 4 BiCGStab, 5 other.  Timing adds events around each class. */
+#define SW2G_NCLASSES 6
+int sw2g_set_profiling(sw2g_model *m, int on);
+int sw2g_get_profile(sw2g_model *m, double *ms, long long *launches);
+int sw2g_reset_profile(sw2g_model *m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

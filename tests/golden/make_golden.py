@@ -1,0 +1,72 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference's own
+compiled SW2 code (oracle/_ref/adh_ref_harness, built by oracle/Makefile from the
+reference sources).  Run it on a machine that has the reference tree:
+
+    make -C oracle all && python tests/golden/make_golden.py
+
+Each fixture is a compressed .npz holding the case inputs (mesh, states, series)
+and what the reference computed for them.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from adh_kraken_b200.mesh import flume_case, small_delaunay_case  # noqa: E402
+from oracle.refio import run_harness  # noqa: E402
+
+
+def perturbed_states(case, seed):
+    rng = np.random.default_rng(seed)
+    V = case.nnodes
+    sol = case.sol0.copy(); sol_old = case.sol0.copy(); sol_older = case.sol0.copy()
+    sol[0::3] += 0.01 * rng.standard_normal(V)
+    sol[1::3] += 0.05 * rng.standard_normal(V)
+    sol[2::3] += 0.05 * rng.standard_normal(V)
+    sol_older[0::3] -= 0.01 * rng.standard_normal(V)
+    return sol, sol_old, sol_older
+
+
+def case_arrays(case):
+    out = {"xyz": case.xyz, "tri": case.tri, "seg": case.seg, "seg_kind": case.seg_kind, "sol0": case.sol0,
+           "dt": case.dt, "nsteps": case.nsteps, "t0": case.t0}
+    for k, (t, v) in case.series.items():
+        out[f"series{k}_t"] = t
+        out[f"series{k}_v"] = v
+    return out
+
+
+def dump_fixture(name, case, seed):
+    sol, sol_old, sol_older = perturbed_states(case, seed)
+    d = run_harness("dump", case, sol=sol, sol_old=sol_old, sol_older=sol_older)
+    arrs = case_arrays(case)
+    arrs.update({"sol": sol, "sol_old": sol_old, "sol_older": sol_older})
+    arrs.update({f"ref_{k}": v for k, v in d.items()})
+    np.savez_compressed(os.path.join(HERE, name), **arrs)
+
+
+def run_fixture(name, case):
+    r = run_harness("run", case)
+    arrs = case_arrays(case)
+    arrs.update({f"ref_{k}": v for k, v in r.items() if k != "step_seconds"})
+    np.savez_compressed(os.path.join(HERE, name), **arrs)
+
+
+def main():
+    dump_fixture("dump_flume_21x6.npz", flume_case(nsteps=1, npx=21, npy=6), seed=11)
+    dump_fixture("dump_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=12)
+    run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
+    run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,90 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures made by
+tests/golden/make_golden.py from the compiled reference)."""
+import numpy as np
+import pytest
+
+from fixtures import load, rel_err
+from oracle.oracle import OracleModel
+
+DUMPS = ["dump_flume_21x6.npz", "dump_wetdry_12.npz"]
+RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz"]
+
+
+@pytest.mark.parametrize("name", DUMPS)
+def test_structure_and_maps(name):
+    case, z = load(name)
+    o = OracleModel(case)
+    assert np.array_equal(o.indptr, z["ref_indptr"])
+    assert np.array_equal(o.cols, z["ref_cols"])
+    V = case.nnodes
+    assert np.array_equal(z["ref_dofmap"].reshape(3, V).T.ravel(), np.arange(3 * V)), "dof = 3*node + var"
+
+
+@pytest.mark.parametrize("name", DUMPS)
+def test_bc_series_average(name):
+    case, z = load(name)
+    o = OracleModel(case)
+    assert np.array_equal(np.array(o.bc_values(case.t0, case.t0 + case.dt)), z["ref_bc_values"])
+
+
+@pytest.mark.parametrize("name", DUMPS)
+def test_element_level_bit_exact(name):
+    case, z = load(name)
+    o = OracleModel(case)
+    sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
+    assert np.array_equal(o.wd_flags(sol, old), z["ref_wd_flag"])
+    et, es = o.elem_resid(sol, old, older)
+    assert np.array_equal(et, z["ref_elem_rhs_tri"])
+    assert np.array_equal(es, z["ref_elem_rhs_seg"])
+    jt, js = o.elem_jac(sol, old, older)
+    assert np.array_equal(jt, z["ref_elem_jac_tri"])
+    assert np.array_equal(js, z["ref_elem_jac_seg"])
+
+
+@pytest.mark.parametrize("name", DUMPS)
+def test_assembly_and_linear_system_bit_exact(name):
+    case, z = load(name)
+    o = OracleModel(case)
+    sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
+    o.wd_flags(sol, old)
+    r = o.residual(sol, old, older)
+    v = o.jacobian(sol, old, older)
+    assert np.array_equal(r, z["ref_residual"])
+    assert np.array_equal(v, z["ref_jac_vals"])
+    bc = np.zeros(o.ndof, np.int32)
+    o.check_diag(v, bc)
+    o.apply_dirichlet(bc, v, r)
+    assert np.array_equal(bc, (z["ref_bc_mask"] == 1).astype(np.int32))
+    assert np.array_equal(v, z["ref_jac_vals_dirichlet"])
+    assert np.array_equal(r, z["ref_residual_dirichlet"])
+    x = np.zeros(o.ndof)
+    s = o.scale_system(v, r, x)
+    assert np.array_equal(s, z["ref_scale_vect"])
+    assert np.array_equal(v, z["ref_jac_vals_scaled"])
+    assert np.array_equal(r, z["ref_residual_scaled"])
+
+
+@pytest.mark.parametrize("name", DUMPS)
+def test_bicgstab_block_jacobi_solves_reference_system(name):
+    """Block-Jacobi BiCGStab reaches the reference's exact-LU solution of the same
+    scaled system to solver tolerance."""
+    case, z = load(name)
+    o = OracleModel(case)
+    v = z["ref_jac_vals_scaled"].copy(); b = z["ref_residual_scaled"].copy(); x = np.zeros(o.ndof)
+    it = o.bicgstab(v, x, b, z["ref_scale_vect"], max_it=20000, tol=1e-13)
+    ref = z["ref_dsol"]
+    assert it > 0
+    # the two preconditioners reach the same solution to the conditioning of the system
+    assert np.abs(x - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_time_steps_match_reference(name):
+    """Several implicit steps with block-Jacobi BiCGStab land on the reference's
+    converged states (exact LU preconditioner) within 1e-8 relative."""
+    case, z = load(name)
+    o = OracleModel(case)
+    sol, hist = o.run(case.nsteps, krylov_max_it=20000)
+    assert all(h["ok"] for h in hist)
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
+    assert max(rel_err(sol, ref)) < 1e-8
