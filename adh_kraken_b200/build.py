@@ -23,6 +23,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = [
     ("sw2_kernels.cu", ["--fmad=false"]),
     ("la_kernels.cu", []),
+    ("ilu_kernels.cu", []),
     ("sw2_capi.cu", []),
 ]
 

@@ -36,7 +36,10 @@ class NewtonOpts(C.Structure):
     _fields_ = [("tol_nonlin", C.c_double), ("inc_nonlin", C.c_double), ("max_nonlin_it", C.c_int),
                 ("max_linesearch_cuts", C.c_int), ("krylov_max_it", C.c_int), ("krylov_tol", C.c_double),
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
-                ("use_guess", C.c_int)]
+                ("use_guess", C.c_int), ("precond", C.c_int)]
+
+PC_BLOCK_JACOBI = 0
+PC_BILU0 = 1
 
 
 class NewtonStats(C.Structure):
@@ -176,11 +179,11 @@ class SW2Model:
         self._check(lib().sw2g_prepare_system(self.h, _d(vals), _d(residual), _d(x), _i(bc_mask), _d(scale)))
         return vals, residual, x, bc_mask, scale
 
-    def bicgstab(self, vals, b, x, scale, max_it=4000, tol=1e-11):
+    def bicgstab(self, vals, b, x, scale, max_it=4000, tol=1e-11, precond=PC_BILU0):
         x = _f64(x).copy(); b = _f64(b).copy()
         it = C.c_int()
         self._check(lib().sw2g_solve_linear_sys_bcgstab(self.h, _d(x), _d(_f64(vals)), _d(b), _d(_f64(scale)),
-                                                        int(max_it), C.c_double(tol), C.byref(it)))
+                                                        int(max_it), C.c_double(tol), int(precond), C.byref(it)))
         return x, b, it.value
 
     def fe_newton(self, sol_old, sol_older, bc_mask, dirichlet=None, opts=None):

@@ -526,3 +526,213 @@ void launch_masked_copy(int n, const int* mask, const double* src, double* dst, 
     k_masked_copy<<<(n + 255) / 256, 256, 0, st>>>(n, mask, src, dst);
 }
 }  // namespace sw2
+
+// ======================================================================
+// BiCGStab with an explicit preconditioner apply (multicolour block ILU).
+// Per iteration: Ap = M^-1 (A p); alpha; s; As = M^-1 (A s); omega, rho, beta;
+// update -- the recurrences of bcgstab_solver.c:210-310.
+namespace sw2 {
+
+int grid_for_nodes(long nodes) { return grid_for(8L * nodes, 256); }
+
+template <class VT>
+__global__ void __launch_bounds__(256) k_spmv(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ x,
+                                              VT* __restrict__ y, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int g8 = threadIdx.x & 7, sub = (threadIdx.x & 31) >> 3;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < A.nnodes; base += nw * 4) {
+        const int a = base + sub;
+        const bool valid = a < A.nnodes;
+        double y0 = 0, y1 = 0, y2 = 0;
+        const int rs = valid ? A.indptr[3 * a] : 0;
+        const int len = valid ? A.indptr[3 * a + 1] - rs : 0;
+        const int s0 = valid ? A.bptr[a] : 0, deg = valid ? A.bptr[a + 1] - s0 : 0;
+        for (int j = g8; j < deg; j += 8) {
+            const int b = A.bcol[s0 + j];
+            const double xb0 = x[3 * b], xb1 = x[3 * b + 1], xb2 = x[3 * b + 2];
+            const VT* v0 = vals + rs + 3 * j;
+            y0 += (double)v0[0] * xb0 + (double)v0[1] * xb1 + (double)v0[2] * xb2;
+            const VT* v1 = v0 + len;
+            y1 += (double)v1[0] * xb0 + (double)v1[1] * xb1 + (double)v1[2] * xb2;
+            const VT* v2 = v1 + len;
+            y2 += (double)v2[0] * xb0 + (double)v2[1] * xb1 + (double)v2[2] * xb2;
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+            y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+        }
+        if (g8 == 0 && valid) { y[3 * a] = (VT)y0; y[3 * a + 1] = (VT)y1; y[3 * a + 2] = (VT)y2; }
+    }
+}
+
+template <class VT>
+__global__ void k_copy(int n, const VT* __restrict__ a, VT* __restrict__ b) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+// r = b - r (r holds M^-1 A x) ; q = p = r ; Ap = 0 ; rnorm, bnorm, rho
+template <class VT>
+__global__ void __launch_bounds__(256) k_bicg_init_pc(int n, KrylovVecs<VT> V, KrylovScalars* S, Reduce R) {
+    __shared__ double sh[8];
+    double rmax = 0, bmax = 0, rr = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const VT r = V.b[i] + (VT)-1 * V.r[i];
+        V.r[i] = r; V.q[i] = r; V.p[i] = r; V.Ap[i] = 0;
+        rmax = fmax(rmax, fabs((double)r)); bmax = fmax(bmax, fabs((double)V.b[i]));
+        rr += (double)r * (double)r;
+    }
+    double v[3];
+    v[0] = block_max<256>(rmax, sh); v[1] = block_max<256>(bmax, sh); v[2] = block_sum<256>(rr, sh);
+    if (last_block(R, v, 3)) {
+        double a = 0, b = 0, c = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) { a = fmax(a, ld_part(R, 4 * k)); b = fmax(b, ld_part(R, 4 * k + 1)); c += ld_part(R, 4 * k + 2); }
+        S->rnorm = a; S->bnorm = b; S->rho = c;
+        S->rhop = 1.0; S->alpha = 1.0; S->omega = 1.0; S->beta = 0.0; S->it = 0; S->status = 0;
+        S->done = (a > (S->tol + b * S->rtol)) ? 0 : 1;
+        if (!isfinite(a) || !isfinite(c)) { S->status = 2; S->done = 1; }
+    }
+}
+
+// gamma = q.Ap ; alpha = rho / gamma
+template <class VT>
+__global__ void __launch_bounds__(256) k_bicg_alpha(int n, KrylovVecs<VT> V, KrylovScalars* S, Reduce R) {
+    if (S->done) return;
+    __shared__ double sh[8];
+    double qa = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        qa += (double)V.q[i] * (double)V.Ap[i];
+    double v[1];
+    v[0] = block_sum<256>(qa, sh);
+    if (last_block(R, v, 1)) {
+        double g = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) g += ld_part(R, 4 * k);
+        S->gamma = g;
+        if (g == 0.0 || !isfinite(g)) { S->status = 1; S->done = 1; }
+        else S->alpha = S->rho / g;
+    }
+}
+
+// omega = As.s / As.As ; rho' = -omega As.q ; beta'
+template <class VT>
+__global__ void __launch_bounds__(256) k_bicg_omega(int n, KrylovVecs<VT> V, KrylovScalars* S, Reduce R) {
+    if (S->done) return;
+    __shared__ double sh[8];
+    double ss = 0, aa = 0, aq = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double z = (double)V.As[i];
+        ss += z * (double)V.s[i]; aa += z * z; aq += z * (double)V.q[i];
+    }
+    double v[3];
+    v[0] = block_sum<256>(ss, sh); v[1] = block_sum<256>(aa, sh); v[2] = block_sum<256>(aq, sh);
+    if (last_block(R, v, 3)) {
+        double a = 0, b = 0, c = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) { a += ld_part(R, 4 * k); b += ld_part(R, 4 * k + 1); c += ld_part(R, 4 * k + 2); }
+        if (b == 0.0) { S->omega = 0.0; S->status = 3; }
+        else {
+            const double om = a / b;
+            S->omega = om; S->rhop = S->rho; S->rho = -1.0 * om * c;
+            S->beta = (S->rho * S->alpha) / (S->rhop * om);
+        }
+    }
+}
+
+template <class VT>
+void launch_bicg_init_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+                         cudaStream_t st) {
+    const int gv = grid_for(A.n, 256);
+    launch_bilu_apply<VT>(A, H, V.vals_pc, V.inv, V.b, st);          // b <- M^-1 b
+    k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                    // x = b
+    k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.x, V.r, nullptr);
+    launch_bilu_apply<VT>(A, H, V.vals_pc, V.inv, V.r, st);           // r <- M^-1 A x
+    k_bicg_init_pc<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
+}
+template <class VT>
+void launch_bicg_iteration_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+                              cudaStream_t st) {
+    const int gv = grid_for(A.n, 256), gs = grid_for_nodes(A.nnodes);
+    const int* done = &S->done;
+    IluHost Hs = H; Hs.view.skip = done;
+    k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.p, V.Ap, done);
+    launch_bilu_apply<VT>(A, Hs, V.vals_pc, V.inv, V.Ap, st);
+    k_bicg_alpha<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
+    k_bicg_s<VT><<<gv, 256, 0, st>>>(A.n, V, S);
+    k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.s, V.As, done);
+    launch_bilu_apply<VT>(A, Hs, V.vals_pc, V.inv, V.As, st);
+    k_bicg_omega<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
+    k_bicg_update<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
+}
+template void launch_bicg_init_pc<double>(const BlockCSR&, const IluHost&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_init_pc<float>(const BlockCSR&, const IluHost&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_iteration_pc<double>(const BlockCSR&, const IluHost&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_iteration_pc<float>(const BlockCSR&, const IluHost&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
+
+}  // namespace sw2
+
+namespace sw2 {
+__global__ void __launch_bounds__(256) k_spmv_sub(BlockCSR A, const double* __restrict__ vals, const double* __restrict__ x,
+                                                  const double* __restrict__ b, double* __restrict__ t) {
+    const int g8 = threadIdx.x & 7, sub = (threadIdx.x & 31) >> 3;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < A.nnodes; base += nw * 4) {
+        const int a = base + sub;
+        const bool valid = a < A.nnodes;
+        double y0 = 0, y1 = 0, y2 = 0;
+        const int rs = valid ? A.indptr[3 * a] : 0;
+        const int len = valid ? A.indptr[3 * a + 1] - rs : 0;
+        const int s0 = valid ? A.bptr[a] : 0, deg = valid ? A.bptr[a + 1] - s0 : 0;
+        for (int j = g8; j < deg; j += 8) {
+            const int bb = A.bcol[s0 + j];
+            const double xb0 = x[3 * bb], xb1 = x[3 * bb + 1], xb2 = x[3 * bb + 2];
+            const double* v0 = vals + rs + 3 * j;
+            y0 += v0[0] * xb0 + v0[1] * xb1 + v0[2] * xb2;
+            const double* v1 = v0 + len;
+            y1 += v1[0] * xb0 + v1[1] * xb1 + v1[2] * xb2;
+            const double* v2 = v1 + len;
+            y2 += v2[0] * xb0 + v2[1] * xb1 + v2[2] * xb2;
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+            y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+        }
+        if (g8 == 0 && valid) { t[3 * a] = b[3 * a] - y0; t[3 * a + 1] = b[3 * a + 1] - y1; t[3 * a + 2] = b[3 * a + 2] - y2; }
+    }
+}
+void launch_spmv_sub(const BlockCSR& A, const double* vals, const double* x, const double* b, double* t, cudaStream_t st) {
+    k_spmv_sub<<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, x, b, t);
+}
+__global__ void k_bj_apply(int nnodes, const double* __restrict__ inv, double* __restrict__ z) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nnodes) return;
+    const double* M = inv + 9 * a;
+    const double z0 = z[3 * a], z1 = z[3 * a + 1], z2 = z[3 * a + 2];
+    z[3 * a] = M[0] * z0 + M[1] * z1 + M[2] * z2;
+    z[3 * a + 1] = M[3] * z0 + M[4] * z1 + M[5] * z2;
+    z[3 * a + 2] = M[6] * z0 + M[7] * z1 + M[8] * z2;
+}
+void launch_bj_apply(int nnodes, const double* inv, double* z, cudaStream_t st) {
+    k_bj_apply<<<(nnodes + 255) / 256, 256, 0, st>>>(nnodes, inv, z);
+}
+__global__ void __launch_bounds__(256) k_maxabs(int n, const double* __restrict__ z, Reduce R) {
+    __shared__ double sh[8];
+    double m = 0, bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = fabs(z[i]);
+        if (!isfinite(a)) bad = 1; else m = fmax(m, a);
+    }
+    double v[2];
+    v[0] = block_max<256>(m, sh); v[1] = block_max<256>(bad, sh);
+    if (last_block(R, v, 2)) {
+        double a = 0, b = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) { a = fmax(a, ld_part(R, 4 * k)); b = fmax(b, ld_part(R, 4 * k + 1)); }
+        R.out[0] = b > 0 ? NAN : a;   // a non-finite entry is reported, not hidden by fmax
+    }
+}
+void launch_maxabs(int n, const double* z, Reduce R, cudaStream_t st) {
+    k_maxabs<<<grid_for(n, 256), 256, 0, st>>>(n, z, R);
+}
+}  // namespace sw2

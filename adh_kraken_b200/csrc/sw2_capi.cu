@@ -73,7 +73,12 @@ struct sw2g_model {
     double *d_partial = nullptr, *d_rout = nullptr; unsigned int* d_counter = nullptr;
     KrylovScalars* d_ks = nullptr;
     double* h_rout = nullptr; KrylovScalars* h_ks = nullptr;
-    cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+    cudaGraphExec_t graph64[2] = {nullptr, nullptr}, graph32[2] = {nullptr, nullptr};   // [precond]
+    // multicolour block ILU(0)
+    std::vector<int> h_color_ptr;
+    int *d_color_nodes = nullptr, *d_node_color = nullptr;
+    double* d_lu = nullptr; float* f_lu = nullptr;
+    IluHost ilu{};
     StepParams P{};
     MeshView M{}; AssemblyMaps A{}; BlockCSR B{};
     // profiling
@@ -158,7 +163,7 @@ static void build_csr(int V, int T, int S, const int* tri, const int* seg, std::
 extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->tol_nonlin = 1e-8; o->inc_nonlin = 1e-6; o->max_nonlin_it = 10; o->max_linesearch_cuts = 5;
     o->krylov_max_it = 4000; o->krylov_tol = 1e-11; o->krylov_precision = 64;
-    o->refine_tol = 1e-6; o->max_refine = 6; o->use_guess = 0;
+    o->refine_tol = 1e-4; o->max_refine = 8; o->use_guess = 0; o->precond = SW2G_PC_BILU0;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -270,6 +275,29 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         blen[k] = ip[3 * a + 1] - ip[3 * a];
     }
 
+    // --- greedy colouring of the node graph for the block-ILU sweeps
+    std::vector<int> color(V, -1);
+    int ncolors = 0;
+    {
+        std::vector<int> seen(64, -1);
+        for (int a = 0; a < V; a++) {
+            if (bptr[a + 1] - bptr[a] > 32) { g_err = "sw2g_create: a node has more than 31 neighbours"; return fail(SW2G_ERR_MESH); }
+            for (int k = bptr[a]; k < bptr[a + 1]; k++) if (color[bcol[k]] >= 0) seen[color[bcol[k]]] = a;
+            int c = 0;
+            while (seen[c] == a) c++;
+            color[a] = c;
+            ncolors = std::max(ncolors, c + 1);
+        }
+    }
+    std::vector<int> color_nodes(V);
+    m->h_color_ptr.assign(ncolors + 1, 0);
+    for (int a = 0; a < V; a++) m->h_color_ptr[color[a] + 1]++;
+    for (int c = 0; c < ncolors; c++) m->h_color_ptr[c + 1] += m->h_color_ptr[c];
+    {
+        std::vector<int> fill(m->h_color_ptr.begin(), m->h_color_ptr.end() - 1);
+        for (int a = 0; a < V; a++) color_nodes[fill[color[a]]++] = a;
+    }
+
     // --- device copies
     if ((rc = upload(m, &m->d_tri, mesh->tri, 3 * (size_t)T))) return fail(rc);
     std::vector<int> segv(2 * (size_t)S + 2, 0), kindv(S + 1, 0);
@@ -288,8 +316,11 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         (rc = upload(m, &m->d_diag, diag.data(), diag.size())) || (rc = upload(m, &m->d_rptr, rptr.data(), rptr.size())) ||
         (rc = upload(m, &m->d_rmap, rmap.data(), rmap.size())) || (rc = upload(m, &m->d_jptr, jptr.data(), jptr.size())) ||
         (rc = upload(m, &m->d_jmap, jmap.data(), jmap.size())) || (rc = upload(m, &m->d_boff, boff.data(), boff.size())) ||
-        (rc = upload(m, &m->d_blen, blen.data(), blen.size())))
+        (rc = upload(m, &m->d_blen, blen.data(), blen.size())) ||
+        (rc = upload(m, &m->d_color_nodes, color_nodes.data(), color_nodes.size())) ||
+        (rc = upload(m, &m->d_node_color, color.data(), color.size())) || (rc = dalloc(m, &m->d_lu, (size_t)m->nnz)))
         return fail(rc);
+    m->ilu = IluHost{ncolors, m->h_color_ptr.data(), IluView{m->d_color_nodes, m->d_node_color, nullptr}};
     const size_t n = m->n;
     if ((rc = dalloc(m, &m->d_sol, n)) || (rc = dalloc(m, &m->d_sol_old, n)) || (rc = dalloc(m, &m->d_sol_older, n)) ||
         (rc = dalloc(m, &m->d_dirichlet, n)) || (rc = dalloc(m, &m->d_guess, n)) || (rc = dalloc(m, &m->d_bc_mask, n)) ||
@@ -328,14 +359,17 @@ static int alloc_fp32(sw2g_model* m) {
     TRY(dalloc(m, &m->f_vals, (size_t)m->nnz)); TRY(dalloc(m, &m->f_inv, 9 * (size_t)m->V));
     TRY(dalloc(m, &m->f_x, n)); TRY(dalloc(m, &m->f_r, n)); TRY(dalloc(m, &m->f_p, n)); TRY(dalloc(m, &m->f_Ap, n));
     TRY(dalloc(m, &m->f_q, n)); TRY(dalloc(m, &m->f_s, n)); TRY(dalloc(m, &m->f_As, n)); TRY(dalloc(m, &m->f_b, n));
+    TRY(dalloc(m, &m->f_lu, (size_t)m->nnz));
     return SW2G_OK;
 }
 
 extern "C" void sw2g_destroy(sw2g_model* m) {
     if (!m) return;
     if (m->st) cudaStreamSynchronize(m->st);
-    if (m->graph64) cudaGraphExecDestroy(m->graph64);
-    if (m->graph32) cudaGraphExecDestroy(m->graph32);
+    for (int k = 0; k < 2; k++) {
+        if (m->graph64[k]) cudaGraphExecDestroy(m->graph64[k]);
+        if (m->graph32[k]) cudaGraphExecDestroy(m->graph32[k]);
+    }
     for (void* p : m->allocs) cudaFree(p);
     if (m->h_rout) cudaFreeHost(m->h_rout);
     if (m->h_ks) cudaFreeHost(m->h_ks);
@@ -408,31 +442,47 @@ static int do_norms(sw2g_model* m, const double* res, const double* dsol, double
 }
 // check_diag + apply_Dirichlet_BC + scale_linear_system on device arrays
 static int do_prepare(sw2g_model* m, double* vals, double* res, double* x) {
-    ProfScope ps(m, 3, 4);
+    ProfScope ps(m, 3, 3);
     launch_check_diag(m->B, vals, m->d_bc_mask, m->st);
     launch_dirichlet_rowscale(m->B, m->d_bc_mask, vals, res, x, m->d_scale, m->st);
     launch_scale_vals(m->B, m->d_scale, vals, m->st);
-    launch_bj_setup(m->B, vals, m->d_inv, m->st);
+    CKL();
+    return SW2G_OK;
+}
+// preconditioner set-up on the scaled matrix (replaces prep_umfpack, bcgstab_solver.c:371)
+static int do_precond_setup(sw2g_model* m, const double* vals, int precond) {
+    if (precond == SW2G_PC_BILU0) {
+        ProfScope ps(m, 3, 1 + m->ilu.ncolors);
+        launch_bilu_factor(m->B, m->ilu, vals, m->d_lu, m->d_inv, m->st);
+    } else {
+        ProfScope ps(m, 3, 1);
+        launch_bj_setup(m->B, vals, m->d_inv, m->st);
+    }
     CKL();
     return SW2G_OK;
 }
 
 template <class VT>
-static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, cudaGraphExec_t* graph, int max_it, double atol, double rtol,
-                    int* iters, int* status) {
+static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_t* graph, int max_it, double atol,
+                    double rtol, int* iters, int* status) {
     KrylovScalars init{};
     init.tol = atol; init.rtol = rtol; init.max_it = max_it;
     Reduce R{m->d_partial, m->d_counter, m->d_rout};
+    const bool ilu = precond == SW2G_PC_BILU0;
     {
-        ProfScope ps(m, 4, 2);
+        ProfScope ps(m, 4, ilu ? 3 + 4 * m->ilu.ncolors : 2);
         CK(cudaMemcpyAsync(m->d_ks, &init, sizeof(KrylovScalars), cudaMemcpyHostToDevice, m->st));
-        launch_bicg_init<VT>(m->B, V, m->d_ks, R, m->st);
+        if (ilu) launch_bicg_init_pc<VT>(m->B, m->ilu, V, m->d_ks, R, m->st);
+        else launch_bicg_init<VT>(m->B, V, m->d_ks, R, m->st);
         CKL();
     }
     if (!*graph) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-        for (int c = 0; c < kChunk; c++) launch_bicg_iteration<VT>(m->B, V, m->d_ks, R, m->st);
+        for (int c = 0; c < kChunk; c++) {
+            if (ilu) launch_bicg_iteration_pc<VT>(m->B, m->ilu, V, m->d_ks, R, m->st);
+            else launch_bicg_iteration<VT>(m->B, V, m->d_ks, R, m->st);
+        }
         cudaError_t e1 = cudaGetLastError();
         cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
         if (e1 != cudaSuccess || e2 != cudaSuccess) {
@@ -442,11 +492,16 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, cudaGraphExec_t* graph, int
         CK(cudaGraphInstantiate(graph, g, 0));
         cudaGraphDestroy(g);
     }
+    const int per_it = ilu ? 6 + 4 * m->ilu.ncolors : 4;
+    static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;   // diagnostic: residual history on stderr
     while (true) {
         CK(cudaMemcpyAsync(m->h_ks, m->d_ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, m->st));
         CK(cudaStreamSynchronize(m->st));
+        if (trace)
+            fprintf(stderr, "krylov it %d rnorm %.3e bnorm %.3e rel %.3e\n", m->h_ks->it, m->h_ks->rnorm, m->h_ks->bnorm,
+                    m->h_ks->rnorm / (m->h_ks->bnorm > 0 ? m->h_ks->bnorm : 1.0));
         if (m->h_ks->done) break;
-        ProfScope ps(m, 4, 4 * kChunk);
+        ProfScope ps(m, 4, per_it * kChunk);
         CK(cudaGraphLaunch(*graph, m->st));
     }
     *iters = m->h_ks->it;
@@ -457,40 +512,48 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, cudaGraphExec_t* graph, int
 // Left-preconditioned BiCGStab of bcgstab_solver.c:65-330 on the prepared (scaled)
 // system in d_vals: x (= dsol) in/out with the reference's x0 shift and unscaling;
 // b is overwritten with M^-1 b as in the reference.
-static int solve64(sw2g_model* m, double* x, double* b, int max_it, double tol, int* iters, int* status) {
+static int solve64(sw2g_model* m, double* x, double* b, int precond, int max_it, double tol, int* iters, int* status) {
     CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * m->n, cudaMemcpyDeviceToDevice, m->st));
-    KrylovVecs<double> V{x, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, b, m->d_vals, m->d_inv};
-    TRY(run_bicg<double>(m, V, &m->graph64, max_it, tol, tol, iters, status));
+    KrylovVecs<double> V{x, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, b, m->d_vals, m->d_inv, m->d_lu};
+    TRY(run_bicg<double>(m, V, precond, &m->graph64[precond == SW2G_PC_BILU0], max_it, tol, tol, iters, status));
     ProfScope ps(m, 5, 1);
     launch_unscale(m->n, m->d_x0, m->d_scale, x, m->st);
     CKL();
     return SW2G_OK;
 }
 
-// FP32 BiCGStab inside FP64 iterative refinement, on the same scaled,
-// block-Jacobi-preconditioned system.  x accumulates in FP64.  Each pass forms the
-// FP64 residual t = b - A x, stops when the reference's test holds for it
-// (max|M^-1 t| <= tol + tol * max|M^-1 b|), and otherwise solves A d = t in FP32
-// to a relative reduction of refine_tol and adds d to x in FP64.
+// FP32 BiCGStab inside FP64 iterative refinement, on the same scaled and
+// preconditioned system.  x accumulates in FP64.  Each pass forms the FP64
+// residual t = b - A x and applies the FP64 preconditioner; the reference's
+// stopping test (max|M^-1 t| <= tol + tol * max|M^-1 b|) ends the refinement;
+// otherwise A d = t is solved in FP32 (matrix, factor and vectors in FP32) to a
+// relative reduction refine_tol and d is added to x in FP64.
 static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& o, int* iters, int* passes, int* status) {
     TRY(alloc_fp32(m));
     const int n = m->n;
+    const bool ilu = o.precond == SW2G_PC_BILU0;
     Reduce R{m->d_partial, m->d_counter, m->d_rout};
     CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_b64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
     CK(cudaMemsetAsync(x, 0, sizeof(double) * n, m->st));
     {
-        ProfScope ps(m, 3, 2);
+        ProfScope ps(m, 3, 3);
         launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
         launch_to_float(9 * m->V, m->d_inv, m->f_inv, m->st);
+        if (ilu) launch_to_float(m->nnz, m->d_lu, m->f_lu, m->st);
         CKL();
     }
     *iters = 0; *passes = 0; *status = 0;
     double bnorm = -1;
+    double* z = m->k_s;   // FP64 Krylov vectors are free in this mode
     for (int pass = 0; pass <= o.max_refine; pass++) {
         {
-            ProfScope ps(m, 4, 1);
-            launch_resid_pnorm(m->B, m->d_vals, m->d_inv, x, m->d_b64, m->d_t64, R, m->st);
+            ProfScope ps(m, 4, 3 + (ilu ? 2 * m->ilu.ncolors : 1));
+            launch_spmv_sub(m->B, m->d_vals, x, m->d_b64, m->d_t64, m->st);
+            CK(cudaMemcpyAsync(z, m->d_t64, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+            if (ilu) launch_bilu_apply<double>(m->B, m->ilu, m->d_lu, m->d_inv, z, m->st);
+            else launch_bj_apply(m->V, m->d_inv, z, m->st);
+            launch_maxabs(n, z, R, m->st);
             CKL();
         }
         CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
@@ -504,9 +567,9 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
             launch_to_float(n, m->d_t64, m->f_b, m->st);
             CKL();
         }
-        KrylovVecs<float> V32{m->f_x, m->f_r, m->f_p, m->f_Ap, m->f_q, m->f_s, m->f_As, m->f_b, m->f_vals, m->f_inv};
+        KrylovVecs<float> V32{m->f_x, m->f_r, m->f_p, m->f_Ap, m->f_q, m->f_s, m->f_As, m->f_b, m->f_vals, m->f_inv, m->f_lu};
         int it = 0, st = 0;
-        TRY(run_bicg<float>(m, V32, &m->graph32, o.krylov_max_it, 0.0, o.refine_tol, &it, &st));
+        TRY(run_bicg<float>(m, V32, o.precond, &m->graph32[ilu], o.krylov_max_it, 0.0, o.refine_tol, &it, &st));
         *iters += it; *passes += 1;
         if (st == 1 || st == 2) *status = st;
         {
@@ -557,9 +620,10 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
         TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
         CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
         TRY(do_prepare(m, m->d_vals, m->d_res, m->d_dsol));
+        TRY(do_precond_setup(m, m->d_vals, o.precond));
         int kit = 0, kst = 0, passes = 0;
         if (o.krylov_precision == 32) TRY(solve32(m, m->d_dsol, m->d_res, o, &kit, &passes, &kst));
-        else TRY(solve64(m, m->d_dsol, m->d_res, o.krylov_max_it, o.krylov_tol, &kit, &kst));
+        else TRY(solve64(m, m->d_dsol, m->d_res, o.precond, o.krylov_max_it, o.krylov_tol, &kit, &kst));
         st.krylov_its += kit; st.refine_passes += passes;
         if (kst == 1 || kst == 2) st.krylov_breakdowns++;
         {   // increment_function (newton_tools.c:261) and dsol = -dsol (fe_newton.c:553-555)
@@ -700,20 +764,17 @@ extern "C" int sw2g_prepare_system(sw2g_model* m, double* vals, double* residual
 }
 
 extern "C" int sw2g_solve_linear_sys_bcgstab(sw2g_model* m, double* x, const double* vals, double* b,
-                                             const double* scale_vect, int max_it, double tol, int* iters) {
-    NEED(m && x && vals && b && scale_vect && max_it >= 0 && tol >= 0, "sw2g_solve_linear_sys_bcgstab: bad argument");
+                                             const double* scale_vect, int max_it, double tol, int precond, int* iters) {
+    NEED(m && x && vals && b && scale_vect && max_it >= 0 && tol >= 0 &&
+         (precond == SW2G_PC_BILU0 || precond == SW2G_PC_BLOCK_JACOBI), "sw2g_solve_linear_sys_bcgstab: bad argument");
     const size_t n = m->n;
     CK(cudaMemcpyAsync(m->d_vals, vals, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_res, b, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_dsol, x, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_scale, scale_vect, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
-    {
-        ProfScope ps(m, 3, 1);
-        launch_bj_setup(m->B, m->d_vals, m->d_inv, m->st);
-        CKL();
-    }
+    TRY(do_precond_setup(m, m->d_vals, precond));
     int it = 0, status = 0;
-    TRY(solve64(m, m->d_dsol, m->d_res, max_it, tol, &it, &status));
+    TRY(solve64(m, m->d_dsol, m->d_res, precond, max_it, tol, &it, &status));
     CK(cudaMemcpyAsync(x, m->d_dsol, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaMemcpyAsync(b, m->d_res, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));

@@ -57,7 +57,8 @@ template <class VT>
 struct KrylovVecs {       // VT: double (FP64 path) or float (FP32 path)
     VT *x, *r, *p, *Ap, *q, *s, *As, *b;
     const VT* vals;       // matrix values in the reference CSR order
-    const VT* inv;        // [nnodes*9] block-Jacobi inverses
+    const VT* inv;        // [nnodes*9] block-Jacobi inverses, or the inverted ILU diagonal blocks
+    const VT* vals_pc;    // block-ILU factor in the CSR layout (unused by block-Jacobi)
 };
 
 template <class VT>
@@ -70,6 +71,37 @@ void launch_resid_pnorm(const BlockCSR& A, const double* vals, const double* inv
                         double* t, Reduce R, cudaStream_t st);
 
 void launch_masked_copy(int n, const int* mask, const double* src, double* dst, cudaStream_t st);
+// ---- multicolour block ILU(0) (ilu_kernels.cu)
+struct IluView {            // device
+    const int* color_nodes; // nodes sorted by (colour, id)
+    const int* node_color;  // [nnodes]
+    const int* skip;        // optional device flag: non-zero makes the sweeps no-ops (a finished solve)
+};
+struct IluHost {
+    int ncolors;
+    const int* color_ptr;   // host [ncolors+1] ranges into color_nodes
+    IluView view;
+};
+void launch_bilu_factor(const BlockCSR& A, const IluHost& H, const double* vals, double* lu, double* dinv,
+                        cudaStream_t st);
+template <class VT>
+void launch_bilu_apply(const BlockCSR& A, const IluHost& H, const VT* lu, const VT* dinv, VT* y, cudaStream_t st);
+int grid_for_nodes(long nodes);   // grid for 8-lanes-per-node kernels
+
+// BiCGStab with an explicit preconditioner apply (block ILU): same scalars and
+// stopping rule as the fused block-Jacobi kernels above.
+template <class VT>
+void launch_bicg_init_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+                         cudaStream_t st);
+template <class VT>
+void launch_bicg_iteration_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+                              cudaStream_t st);
+
+// FP64 refinement helpers: t = b - A x ; z <- M^-1 z (block-Jacobi) ; out[0] = max |z|
+void launch_spmv_sub(const BlockCSR& A, const double* vals, const double* x, const double* b, double* t, cudaStream_t st);
+void launch_bj_apply(int nnodes, const double* inv, double* z, cudaStream_t st);
+void launch_maxabs(int n, const double* z, Reduce R, cudaStream_t st);
+
 void launch_unscale(int n, const double* x0, const double* scale, double* x, cudaStream_t st);
 void launch_axpy(int n, double a, const double* x, double* y, cudaStream_t st);   // y += a x
 void launch_scal(int n, double a, double* x, cudaStream_t st);                    // x *= a

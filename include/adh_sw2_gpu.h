@@ -55,7 +55,12 @@ typedef struct {
     double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
     int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
     int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess instead of sol_old */
+    int precond;              /* SW2G_PC_BILU0 (default) or SW2G_PC_BLOCK_JACOBI */
 } sw2g_newton_opts;
+
+/* preconditioners standing in for the reference's full UMFPACK LU (bcgstab_solver.c:371-420) */
+#define SW2G_PC_BLOCK_JACOBI 0   /* 3x3 nodal block-Jacobi */
+#define SW2G_PC_BILU0 1          /* multicolour 3x3 block ILU(0) over the node graph */
 
 typedef struct {
     int newton_its;           /* Newton iterations of the step */
@@ -112,10 +117,10 @@ int sw2g_assemble_jacobian(sw2g_model *m, const double *sol, const double *sol_o
 int sw2g_prepare_system(sw2g_model *m, double *vals, double *residual, double *x, int *bc_mask, double *scale);
 /* solve_linear_sys_bcgstab (src/la/la.h:22-29), serial branch: x in/out (the x0 shift
  * and the unscaling are the reference's), b is overwritten with M^-1 b as in the
- * reference.  The exact UMFPACK LU preconditioner is replaced by 3x3 nodal
- * block-Jacobi.  Returns the iteration count in *iters. */
+ * reference.  The exact UMFPACK LU preconditioner is replaced by `precond`
+ * (SW2G_PC_*).  Returns the iteration count in *iters (negative on breakdown). */
 int sw2g_solve_linear_sys_bcgstab(sw2g_model *m, double *x, const double *vals, double *b, const double *scale_vect,
-                                  int max_it, double tol, int *iters);
+                                  int max_it, double tol, int precond, int *iters);
 /* fe_newton(SMODEL_SUPER*) (src/newton/newton.h:19) for one time step: sol out;
  * sol_old/sol_older in; bc_mask in/out (permanent Dirichlet marks); dirichlet in. */
 int sw2g_fe_newton(sw2g_model *m, double *sol, const double *sol_old, const double *sol_older, int *bc_mask,
