@@ -24,6 +24,8 @@ UNITS = [
     ("sw2_kernels.cu", ["--fmad=false"]),
     ("la_kernels.cu", []),
     ("ilu_kernels.cu", []),
+    ("amg_kernels.cu", []),
+    ("gmres_kernels.cu", []),
     ("sw2_capi.cu", []),
 ]
 

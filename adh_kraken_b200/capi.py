@@ -23,7 +23,7 @@ EXPORTED = [
     "sw2g_set_step", "sw2g_wd_flags", "sw2g_elem_resid", "sw2g_elem_jac", "sw2g_assemble_residual",
     "sw2g_assemble_jacobian", "sw2g_prepare_system", "sw2g_solve_linear_sys_bcgstab", "sw2g_fe_newton",
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
-    "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile",
+    "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
 ]
 
 
@@ -36,10 +36,13 @@ class NewtonOpts(C.Structure):
     _fields_ = [("tol_nonlin", C.c_double), ("inc_nonlin", C.c_double), ("max_nonlin_it", C.c_int),
                 ("max_linesearch_cuts", C.c_int), ("krylov_max_it", C.c_int), ("krylov_tol", C.c_double),
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
-                ("use_guess", C.c_int), ("precond", C.c_int)]
+                ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int)]
 
 PC_BLOCK_JACOBI = 0
 PC_BILU0 = 1
+PC_AMG = 2
+KRYLOV_BICGSTAB = 0
+KRYLOV_GMRES = 1
 
 
 class NewtonStats(C.Structure):
@@ -179,7 +182,7 @@ class SW2Model:
         self._check(lib().sw2g_prepare_system(self.h, _d(vals), _d(residual), _d(x), _i(bc_mask), _d(scale)))
         return vals, residual, x, bc_mask, scale
 
-    def bicgstab(self, vals, b, x, scale, max_it=4000, tol=1e-11, precond=PC_BILU0):
+    def bicgstab(self, vals, b, x, scale, max_it=4000, tol=1e-11, precond=PC_AMG):
         x = _f64(x).copy(); b = _f64(b).copy()
         it = C.c_int()
         self._check(lib().sw2g_solve_linear_sys_bcgstab(self.h, _d(x), _d(_f64(vals)), _d(b), _d(_f64(scale)),
@@ -237,6 +240,13 @@ class SW2Model:
 
     def reset_profile(self):
         self._check(lib().sw2g_reset_profile(self.h))
+
+    def time_kernel(self, which, reps=20):
+        """(mean ms per launch, algorithmic bytes per launch) of kernel family `which`:
+        0 FP64 SpMV, 1 FD Jacobian, 2 element residual, 3 Jacobian gather, 4 AMG smoothing sweep."""
+        ms, by = C.c_double(), C.c_double()
+        self._check(lib().sw2g_time_kernel(self.h, int(which), int(reps), C.byref(ms), C.byref(by)))
+        return ms.value, by.value
 
 
 def _f64(a):

@@ -1,0 +1,245 @@
+// One cycle of right-preconditioned GMRES(m) on the scaled SW2 system, entirely
+// on the device so that a cycle is one CUDA graph replay.
+//
+// Why next to the reference's BiCGStab: with an approximate multilevel
+// preconditioner the preconditioned SW2 operator at large Courant numbers is far
+// from normal, and BiCGStab's residual then swings by orders of magnitude (in
+// FP32 it does not recover).  GMRES minimises the residual over the Krylov space,
+// so it decreases monotonically; restarted from the true FP64 residual after each
+// cycle it serves both the FP64 solve and the FP32 inner solve of the iterative
+// refinement.
+//
+// A cycle from x = 0 on right-hand side r:
+//   beta = ||r||_2, v_0 = r / beta, g = beta e_0
+//   for j < m:  w = A M^-1 v_j ; h_{:,j} = V_j^T w (one multi-dot pass) ;
+//               w -= V_j h_{:,j} ; h_{j+1,j} = ||w|| ; v_{j+1} = w / h_{j+1,j} ;
+//               Givens rotation of column j ; stop when |g_{j+1}| <= rtol * beta
+//   y = H^-1 g (k x k triangular), out = M^-1 (V_k y)
+// Classical Gram-Schmidt keeps one pass over the basis per step; its dot products
+// accumulate in FP64 whatever the basis precision.  The rotations and the
+// triangular solve run in one thread (k <= kGmM).  Deterministic: fixed block
+// order in every reduction, no atomics besides the last-block counter.
+#include <cmath>
+#include "sw2_launch.h"
+
+namespace sw2 {
+
+static int gm_grid(long n) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0; cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    long need = (n + 255) / 256, cap = 4L * sms;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    return (int)(need < cap ? (need < 1 ? 1 : need) : cap);
+}
+
+// last block of the grid (thread 0) after every block published its partials
+__device__ __forceinline__ bool gm_last_block(const GmresDev& G) {
+    __shared__ bool is_last;
+    __threadfence();   // every thread's partial writes are visible device-wide before the count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = atomicInc(G.counter, gridDim.x - 1);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return is_last;
+}
+
+// beta = ||r||_2 ; g = beta e_0 ; target = rtol * beta ; columns = 0
+template <class VT>
+__global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ r, GmresDev G) {
+    __shared__ double sh[8];
+    double ss = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = r[i];
+        ss += v * v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < 8; k++) t += sh[k];
+        G.partial[blockIdx.x * (kGmM + 1)] = t;
+    }
+    if (gm_last_block(G) && threadIdx.x == 0) {
+        double t = 0;
+        for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1));
+        const double beta = sqrt(t);
+        G.scal[0] = beta;
+        G.scal[1] = G.scal[3] * beta;       // stopping target on |g_{j+1}|
+        G.scal[2] = beta;
+        for (int k = 0; k <= kGmM; k++) G.g[k] = 0.0;
+        G.g[0] = beta;
+        G.state[1] = 0;
+        G.state[2] = isfinite(beta) ? 0 : 2;
+        G.state[0] = (beta > 0.0 && isfinite(beta)) ? 0 : 1;
+    }
+}
+
+template <class VT>
+__global__ void k_gm_v0(int n, const VT* __restrict__ r, VT* __restrict__ v0, GmresDev G) {
+    if (G.state[0]) return;
+    const double inv = 1.0 / G.scal[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v0[i] = (VT)((double)r[i] * inv);
+}
+
+// h_k = v_k . w for k < nv (w = v_nv before orthogonalisation), into column j of H
+template <class VT>
+__global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __restrict__ Vb, size_t ld, int j, GmresDev G) {
+    if (G.state[0]) return;
+    __shared__ double sh[8][kGmM + 1];
+    const VT* w = Vb + (size_t)nv * ld;
+    double acc[kGmM + 1];
+#pragma unroll
+    for (int k = 0; k <= kGmM; k++) acc[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int k = 0; k <= kGmM; k++)
+            if (k < nv) acc[k] += (double)Vb[(size_t)k * ld + i] * wi;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k <= kGmM; k++) {
+        if (k < nv) {
+            double v = acc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sh[warp][k] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double t = 0;
+        for (int w8 = 0; w8 < 8; w8++) t += sh[w8][threadIdx.x];
+        G.partial[blockIdx.x * (kGmM + 1) + threadIdx.x] = t;
+    }
+    if (gm_last_block(G)) {
+        if (threadIdx.x < nv) {
+            double t = 0;
+            for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1) + threadIdx.x);
+            G.H[j * (kGmM + 1) + threadIdx.x] = t;
+        }
+    }
+}
+
+// w -= sum_k h_k v_k ; h_{j+1,j} = ||w|| ; Givens rotation of column j ; convergence test
+template <class VT>
+__global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ Vb, size_t ld, GmresDev G) {
+    if (G.state[0]) return;
+    __shared__ double sh[8];
+    __shared__ double h[kGmM + 1];
+    if (threadIdx.x <= j) h[threadIdx.x] = __ldcg(G.H + j * (kGmM + 1) + threadIdx.x);
+    __syncthreads();
+    VT* w = Vb + (size_t)(j + 1) * ld;
+    double ss = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = w[i];
+        for (int k = 0; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
+        const VT vv = (VT)v;
+        w[i] = vv;
+        ss += (double)vv * (double)vv;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int k = 0; k < 8; k++) t += sh[k];
+        G.partial[blockIdx.x * (kGmM + 1)] = t;
+    }
+    if (gm_last_block(G) && threadIdx.x == 0) {
+        double t = 0;
+        for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1));
+        const double hn = sqrt(t);
+        double* col = G.H + j * (kGmM + 1);
+        for (int k = 0; k < j; k++) {                 // earlier rotations
+            const double a = col[k], b = col[k + 1];
+            col[k] = G.cs[k] * a + G.sn[k] * b;
+            col[k + 1] = -G.sn[k] * a + G.cs[k] * b;
+        }
+        const double a = col[j], b = hn;
+        const double rr = hypot(a, b);
+        const double c = rr > 0.0 ? a / rr : 1.0, s = rr > 0.0 ? b / rr : 0.0;
+        G.cs[j] = c; G.sn[j] = s;
+        col[j] = rr; col[j + 1] = 0.0;
+        G.g[j + 1] = -s * G.g[j];
+        G.g[j] = c * G.g[j];
+        G.scal[4] = hn;
+        G.scal[2] = fabs(G.g[j + 1]);
+        G.state[1] = j + 1;
+        if (!isfinite(rr) || !isfinite(hn)) { G.state[2] = 2; G.state[0] = 1; G.state[1] = j; }
+        else if (rr == 0.0) { G.state[2] = 1; G.state[0] = 1; G.state[1] = j; }   // breakdown: drop column j
+        else if (!(fabs(G.g[j + 1]) > G.scal[1]) || hn == 0.0) G.state[0] = 1;
+    }
+}
+
+template <class VT>
+__global__ void k_gm_scale(int n, int j, VT* __restrict__ Vb, size_t ld, GmresDev G) {
+    if (G.state[0]) return;
+    const double inv = 1.0 / G.scal[4];
+    VT* w = Vb + (size_t)(j + 1) * ld;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = (VT)((double)w[i] * inv);
+}
+
+// y = H^-1 g on the k columns built (upper triangular after the rotations)
+__global__ void k_gm_solve(GmresDev G) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int k = G.state[1];
+    for (int i = k - 1; i >= 0; i--) {
+        double s = G.g[i];
+        for (int t = i + 1; t < k; t++) s -= G.H[t * (kGmM + 1) + i] * G.y[t];
+        const double d = G.H[i * (kGmM + 1) + i];
+        G.y[i] = d != 0.0 ? s / d : 0.0;
+    }
+    G.state[0] = 0;   // let the final preconditioner apply run
+}
+
+// out = V_k y
+template <class VT>
+__global__ void k_gm_combine(int n, const VT* __restrict__ Vb, size_t ld, VT* __restrict__ out, GmresDev G) {
+    __shared__ double y[kGmM];
+    const int k = G.state[1];
+    if (threadIdx.x < k) y[threadIdx.x] = G.y[threadIdx.x];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int t = 0; t < k; t++) s += y[t] * (double)Vb[(size_t)t * ld + i];
+        out[i] = (VT)s;
+    }
+}
+
+template <class VT>
+void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
+                 VT* out, const GmresDev& G, cudaStream_t st) {
+    const int n = A.n, g = gm_grid(n);
+    const int* done = G.state;
+    k_gm_start<VT><<<g, 256, 0, st>>>(n, rhs, G);
+    k_gm_v0<VT><<<g, 256, 0, st>>>(n, rhs, Vb, G);
+    for (int j = 0; j < kGmM; j++) {
+        VT* vj = Vb + (size_t)j * ld;
+        VT* w = Vb + (size_t)(j + 1) * ld;
+        copy_skip<VT>(n, vj, z, done, st);
+        precond_apply<VT>(A, P, z, done, st);
+        spmv_skip<VT>(A, vals, z, w, done, st);
+        k_gm_dots<VT><<<g, 256, 0, st>>>(n, j + 1, Vb, ld, j, G);
+        k_gm_orth<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+        k_gm_scale<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+    }
+    k_gm_solve<<<1, 32, 0, st>>>(G);
+    k_gm_combine<VT><<<g, 256, 0, st>>>(n, Vb, ld, out, G);
+    precond_apply<VT>(A, P, out, nullptr, st);
+}
+template void gmres_cycle<double>(const BlockCSR&, const PrecondOp<double>&, const double*, double*, size_t, double*,
+                                  const double*, double*, const GmresDev&, cudaStream_t);
+template void gmres_cycle<float>(const BlockCSR&, const PrecondOp<float>&, const float*, float*, size_t, float*,
+                                 const float*, float*, const GmresDev&, cudaStream_t);
+
+}  // namespace sw2

@@ -371,7 +371,7 @@ template <class VT>
 __global__ void __launch_bounds__(256) k_bicg_update(int n, KrylovVecs<VT> V, KrylovScalars* S, Reduce R) {
     if (S->done) return;
     __shared__ double sh[8];
-    const bool s_zero = S->status == 3;
+    const bool s_zero = S->status == 3 || S->status == 5;
     const VT alpha = (VT)S->alpha, omega = (VT)S->omega, beta = (VT)S->beta;
     double rmax = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(256) k_bicg_update(int n, KrylovVecs<VT> V, Kr
         S->rnorm = m;
         S->it += 1;
         if (S->status == 3) { S->status = 0; S->done = 1; }
+        if (S->status == 5) { S->status = 1; S->done = 1; }
         if (!(m > (S->tol + S->bnorm * S->rtol)) || S->it >= S->max_it) S->done = 1;
         if (!isfinite(m)) { S->status = 2; S->done = 1; }
     }
@@ -633,41 +634,106 @@ __global__ void __launch_bounds__(256) k_bicg_omega(int n, KrylovVecs<VT> V, Kry
         if (b == 0.0) { S->omega = 0.0; S->status = 3; }
         else {
             const double om = a / b;
-            S->omega = om; S->rhop = S->rho; S->rho = -1.0 * om * c;
-            S->beta = (S->rho * S->alpha) / (S->rhop * om);
+            const double rho_new = -1.0 * om * c;
+            const double beta = (rho_new * S->alpha) / (S->rho * om);
+            if (om == 0.0 || rho_new == 0.0 || !isfinite(om) || !isfinite(beta)) {
+                S->omega = 0.0; S->status = 5;   // breakdown: take the half step x += alpha p, then stop
+            } else {
+                S->omega = om; S->rhop = S->rho; S->rho = rho_new; S->beta = beta;
+            }
         }
     }
 }
 
+void launch_spmv64(const BlockCSR& A, const double* vals, const double* x, double* y, cudaStream_t st) {
+    k_spmv<double><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, x, y, nullptr);
+}
+
 template <class VT>
-void launch_bicg_init_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st) {
+    if (P.kind == 2) {
+        amg_apply<VT>(A, *P.amg, P.vals, y, skip, st);
+    } else {
+        IluHost Hs = *P.ilu; Hs.view.skip = skip;
+        launch_bilu_apply<VT>(A, Hs, P.lu, P.dinv, y, st);
+    }
+}
+template void precond_apply<double>(const BlockCSR&, const PrecondOp<double>&, double*, const int*, cudaStream_t);
+template void precond_apply<float>(const BlockCSR&, const PrecondOp<float>&, float*, const int*, cudaStream_t);
+
+template <class VT>
+__global__ void k_copy_skip(int n, const VT* __restrict__ a, VT* __restrict__ b, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+// Left preconditioning (the reference's form, bcgstab_solver.c:65-330): the
+// recurrences run on M^-1 A and M^-1 b, so the stopping test sees preconditioned
+// residuals.  Right preconditioning runs the same recurrences on A M^-1 with the
+// plain b (x holds y, and x = M^-1 y is taken after the loop), so the stopping
+// test sees the true residual of the scaled system -- needed when M is an
+// approximate multilevel operator whose M^-1 r can be small while r is not.  Both
+// start from x0 = M^-1 b.
+template <class VT>
+void launch_bicg_init_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
                          cudaStream_t st) {
     const int gv = grid_for(A.n, 256);
-    launch_bilu_apply<VT>(A, H, V.vals_pc, V.inv, V.b, st);          // b <- M^-1 b
-    k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                    // x = b
-    k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.x, V.r, nullptr);
-    launch_bilu_apply<VT>(A, H, V.vals_pc, V.inv, V.r, st);           // r <- M^-1 A x
+    if (P.right) {
+        k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                // y = b
+        k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.x, V.z);
+        precond_apply<VT>(A, P, V.z, nullptr, st);                    // z = M^-1 y
+        k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.z, V.r, nullptr);
+    } else {
+        precond_apply<VT>(A, P, V.b, nullptr, st);                    // b <- M^-1 b
+        k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                // x = b
+        k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.x, V.r, nullptr);
+        precond_apply<VT>(A, P, V.r, nullptr, st);                    // r <- M^-1 A x
+    }
     k_bicg_init_pc<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
 }
 template <class VT>
-void launch_bicg_iteration_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+void copy_skip(int n, const VT* a, VT* b, const int* skip, cudaStream_t st) {
+    k_copy_skip<VT><<<grid_for(n, 256), 256, 0, st>>>(n, a, b, skip);
+}
+template <class VT>
+void spmv_skip(const BlockCSR& A, const VT* vals, const VT* x, VT* y, const int* skip, cudaStream_t st) {
+    k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, x, y, skip);
+}
+template void copy_skip<double>(int, const double*, double*, const int*, cudaStream_t);
+template void copy_skip<float>(int, const float*, float*, const int*, cudaStream_t);
+template void spmv_skip<double>(const BlockCSR&, const double*, const double*, double*, const int*, cudaStream_t);
+template void spmv_skip<float>(const BlockCSR&, const float*, const float*, float*, const int*, cudaStream_t);
+
+template <class VT>
+void launch_bicg_iteration_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
                               cudaStream_t st) {
     const int gv = grid_for(A.n, 256), gs = grid_for_nodes(A.nnodes);
     const int* done = &S->done;
-    IluHost Hs = H; Hs.view.skip = done;
-    k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.p, V.Ap, done);
-    launch_bilu_apply<VT>(A, Hs, V.vals_pc, V.inv, V.Ap, st);
+    if (P.right) {
+        k_copy_skip<VT><<<gv, 256, 0, st>>>(A.n, V.p, V.z, done);
+        precond_apply<VT>(A, P, V.z, done, st);
+        k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.z, V.Ap, done);
+    } else {
+        k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.p, V.Ap, done);
+        precond_apply<VT>(A, P, V.Ap, done, st);
+    }
     k_bicg_alpha<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
     k_bicg_s<VT><<<gv, 256, 0, st>>>(A.n, V, S);
-    k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.s, V.As, done);
-    launch_bilu_apply<VT>(A, Hs, V.vals_pc, V.inv, V.As, st);
+    if (P.right) {
+        k_copy_skip<VT><<<gv, 256, 0, st>>>(A.n, V.s, V.z, done);
+        precond_apply<VT>(A, P, V.z, done, st);
+        k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.z, V.As, done);
+    } else {
+        k_spmv<VT><<<gs, 256, 0, st>>>(A, V.vals, V.s, V.As, done);
+        precond_apply<VT>(A, P, V.As, done, st);
+    }
     k_bicg_omega<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
     k_bicg_update<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
 }
-template void launch_bicg_init_pc<double>(const BlockCSR&, const IluHost&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
-template void launch_bicg_init_pc<float>(const BlockCSR&, const IluHost&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
-template void launch_bicg_iteration_pc<double>(const BlockCSR&, const IluHost&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
-template void launch_bicg_iteration_pc<float>(const BlockCSR&, const IluHost&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_init_pc<double>(const BlockCSR&, const PrecondOp<double>&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_init_pc<float>(const BlockCSR&, const PrecondOp<float>&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_iteration_pc<double>(const BlockCSR&, const PrecondOp<double>&, KrylovVecs<double>, KrylovScalars*, Reduce, cudaStream_t);
+template void launch_bicg_iteration_pc<float>(const BlockCSR&, const PrecondOp<float>&, KrylovVecs<float>, KrylovScalars*, Reduce, cudaStream_t);
 
 }  // namespace sw2
 

@@ -66,19 +66,28 @@ struct sw2g_model {
     int *d_wd = nullptr, *d_node_tmp = nullptr;
     double *d_ER = nullptr, *d_EJ = nullptr, *d_res = nullptr, *d_vals = nullptr, *d_dsol = nullptr;
     double *d_scale = nullptr, *d_inv = nullptr, *d_x0 = nullptr, *d_b64 = nullptr, *d_t64 = nullptr;
-    double *k_r = nullptr, *k_p = nullptr, *k_Ap = nullptr, *k_q = nullptr, *k_s = nullptr, *k_As = nullptr;
+    double *k_r = nullptr, *k_p = nullptr, *k_Ap = nullptr, *k_q = nullptr, *k_s = nullptr, *k_As = nullptr, *k_z = nullptr;
+    double *k_xi = nullptr;   // correction of one restarted pass
     float *f_vals = nullptr, *f_inv = nullptr, *f_x = nullptr, *f_r = nullptr, *f_p = nullptr, *f_Ap = nullptr;
-    float *f_q = nullptr, *f_s = nullptr, *f_As = nullptr, *f_b = nullptr;
+    float *f_q = nullptr, *f_s = nullptr, *f_As = nullptr, *f_b = nullptr, *f_z = nullptr;
     // reductions / scalars
     double *d_partial = nullptr, *d_rout = nullptr; unsigned int* d_counter = nullptr;
     KrylovScalars* d_ks = nullptr;
     double* h_rout = nullptr; KrylovScalars* h_ks = nullptr;
-    cudaGraphExec_t graph64[2] = {nullptr, nullptr}, graph32[2] = {nullptr, nullptr};   // [precond]
+    cudaGraphExec_t graph64[3] = {nullptr, nullptr, nullptr}, graph32[3] = {nullptr, nullptr, nullptr};   // [precond]
     // multicolour block ILU(0)
     std::vector<int> h_color_ptr;
     int *d_color_nodes = nullptr, *d_node_color = nullptr;
     double* d_lu = nullptr; float* f_lu = nullptr;
     IluHost ilu{};
+    // aggregation AMG (hierarchy built on first use)
+    AmgHost amg{};
+    bool amg_ready = false;
+    // restarted GMRES (allocated on first use)
+    GmresDev gm{};
+    double* gm_V64 = nullptr; float* gm_V32 = nullptr;
+    cudaGraphExec_t gm_graph64 = nullptr, gm_graph32 = nullptr;
+    std::vector<int> h_bptr, h_bcol;   // node graph, kept for the AMG set-up
     StepParams P{};
     MeshView M{}; AssemblyMaps A{}; BlockCSR B{};
     // profiling
@@ -163,7 +172,8 @@ static void build_csr(int V, int T, int S, const int* tri, const int* seg, std::
 extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->tol_nonlin = 1e-8; o->inc_nonlin = 1e-6; o->max_nonlin_it = 10; o->max_linesearch_cuts = 5;
     o->krylov_max_it = 4000; o->krylov_tol = 1e-11; o->krylov_precision = 64;
-    o->refine_tol = 1e-4; o->max_refine = 8; o->use_guess = 0; o->precond = SW2G_PC_BILU0;
+    o->refine_tol = 1e-4; o->max_refine = 8; o->use_guess = 0; o->precond = SW2G_PC_AMG;
+    o->krylov_method = SW2G_KRYLOV_GMRES;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -230,6 +240,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         for (int j = 0; j < len / 3; j++) bcol.push_back(cl[ip[3 * a] + 3 * j] / 3);
     }
     m->nslots = bptr[V];
+    m->h_bptr = bptr; m->h_bcol = bcol;
     for (int r = 0; r < m->n; r++) {
         int a = r / 3, j = (int)(std::lower_bound(bcol.begin() + bptr[a], bcol.begin() + bptr[a + 1], a) - bcol.begin()) - bptr[a];
         diag[r] = ip[r] + 3 * j + r % 3;
@@ -328,9 +339,10 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         (rc = dalloc(m, &m->d_ER, 9 * (size_t)m->Etot)) || (rc = dalloc(m, &m->d_EJ, 81 * (size_t)m->Etot)) ||
         (rc = dalloc(m, &m->d_res, n)) || (rc = dalloc(m, &m->d_vals, (size_t)m->nnz)) || (rc = dalloc(m, &m->d_dsol, n)) ||
         (rc = dalloc(m, &m->d_scale, n)) || (rc = dalloc(m, &m->d_inv, 9 * (size_t)V)) || (rc = dalloc(m, &m->d_x0, n)) ||
-        (rc = dalloc(m, &m->d_b64, n)) || (rc = dalloc(m, &m->d_t64, n)) ||
+        (rc = dalloc(m, &m->d_b64, n)) || (rc = dalloc(m, &m->d_t64, 2 * (size_t)n)) ||
         (rc = dalloc(m, &m->k_r, n)) || (rc = dalloc(m, &m->k_p, n)) || (rc = dalloc(m, &m->k_Ap, n)) ||
         (rc = dalloc(m, &m->k_q, n)) || (rc = dalloc(m, &m->k_s, n)) || (rc = dalloc(m, &m->k_As, n)) ||
+        (rc = dalloc(m, &m->k_z, n)) || (rc = dalloc(m, &m->k_xi, n)) ||
         (rc = dalloc(m, &m->d_partial, 4 * (size_t)kMaxBlocks)) || (rc = dalloc(m, &m->d_rout, 8)) ||
         (rc = dalloc(m, &m->d_counter, 1)) || (rc = dalloc(m, &m->d_ks, 1)))
         return fail(rc);
@@ -359,6 +371,7 @@ static int alloc_fp32(sw2g_model* m) {
     TRY(dalloc(m, &m->f_vals, (size_t)m->nnz)); TRY(dalloc(m, &m->f_inv, 9 * (size_t)m->V));
     TRY(dalloc(m, &m->f_x, n)); TRY(dalloc(m, &m->f_r, n)); TRY(dalloc(m, &m->f_p, n)); TRY(dalloc(m, &m->f_Ap, n));
     TRY(dalloc(m, &m->f_q, n)); TRY(dalloc(m, &m->f_s, n)); TRY(dalloc(m, &m->f_As, n)); TRY(dalloc(m, &m->f_b, n));
+    TRY(dalloc(m, &m->f_z, n));
     TRY(dalloc(m, &m->f_lu, (size_t)m->nnz));
     return SW2G_OK;
 }
@@ -366,10 +379,12 @@ static int alloc_fp32(sw2g_model* m) {
 extern "C" void sw2g_destroy(sw2g_model* m) {
     if (!m) return;
     if (m->st) cudaStreamSynchronize(m->st);
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 3; k++) {
         if (m->graph64[k]) cudaGraphExecDestroy(m->graph64[k]);
         if (m->graph32[k]) cudaGraphExecDestroy(m->graph32[k]);
     }
+    if (m->gm_graph64) cudaGraphExecDestroy(m->gm_graph64);
+    if (m->gm_graph32) cudaGraphExecDestroy(m->gm_graph32);
     for (void* p : m->allocs) cudaFree(p);
     if (m->h_rout) cudaFreeHost(m->h_rout);
     if (m->h_ks) cudaFreeHost(m->h_ks);
@@ -449,8 +464,16 @@ static int do_prepare(sw2g_model* m, double* vals, double* res, double* x) {
     CKL();
     return SW2G_OK;
 }
+static int build_amg(sw2g_model* m);
 // preconditioner set-up on the scaled matrix (replaces prep_umfpack, bcgstab_solver.c:371)
 static int do_precond_setup(sw2g_model* m, const double* vals, int precond) {
+    if (precond == SW2G_PC_AMG) {
+        if (!m->amg_ready) TRY(build_amg(m));
+        ProfScope ps(m, 3, 1 + 4 * (m->amg.nlev - 1));
+        amg_setup(m->B, m->amg, m->A, vals, m->st);
+        CKL();
+        return SW2G_OK;
+    }
     if (precond == SW2G_PC_BILU0) {
         ProfScope ps(m, 3, 1 + m->ilu.ncolors);
         launch_bilu_factor(m->B, m->ilu, vals, m->d_lu, m->d_inv, m->st);
@@ -462,17 +485,153 @@ static int do_precond_setup(sw2g_model* m, const double* vals, int precond) {
     return SW2G_OK;
 }
 
+// ------------------------------------------------------------------ AMG hierarchy
+// Structure of the aggregation hierarchy, built once per mesh on the host; the
+// values are recomputed on the device every Newton iteration by amg_setup.
+// Aggregation (greedy, node order): a node whose neighbours are all unassigned
+// starts an aggregate with its whole neighbourhood; the leftovers join the
+// aggregate of their first assigned neighbour.  Level 0 aggregates the node graph
+// of the reference CSR; each coarser level aggregates the previous level's
+// block graph, until at most kAmgCoarsest nodes remain.
+static int aggregate_nodes(int n, const std::vector<int>& gp, const std::vector<int>& gc, std::vector<int>& agg) {
+    agg.assign(n, -1);
+    int na = 0;
+    for (int i = 0; i < n; i++) {
+        if (agg[i] >= 0) continue;
+        bool free_ = true;
+        for (int q = gp[i]; q < gp[i + 1]; q++) if (agg[gc[q]] >= 0) { free_ = false; break; }
+        if (!free_) continue;
+        for (int q = gp[i]; q < gp[i + 1]; q++) agg[gc[q]] = na;
+        agg[i] = na++;
+    }
+    for (int i = 0; i < n; i++) {
+        if (agg[i] >= 0) continue;
+        for (int q = gp[i]; q < gp[i + 1]; q++) if (agg[gc[q]] >= 0) { agg[i] = agg[gc[q]]; break; }
+        if (agg[i] < 0) agg[i] = na++;
+    }
+    return na;
+}
+
+static int build_amg(sw2g_model* m) {
+    struct HostLev { int n; std::vector<int> bptr, bcol, dpos; };
+    struct HostLink { std::vector<int> agg, mptr, mem, gptr, gsrc; };
+    std::vector<HostLev> L(1);
+    std::vector<HostLink> K;
+    L[0].n = m->V; L[0].bptr = m->h_bptr; L[0].bcol = m->h_bcol;
+    while ((L.back().n > kAmgCoarsest || L.size() == 1) && (int)L.size() < kAmgMaxLevels) {
+        const HostLev& F = L.back();
+        HostLink lk;
+        const int nc = aggregate_nodes(F.n, F.bptr, F.bcol, lk.agg);
+        if (nc >= F.n) break;   // nothing left to coarsen
+        lk.mptr.assign(nc + 1, 0);
+        for (int i = 0; i < F.n; i++) lk.mptr[lk.agg[i] + 1]++;
+        for (int I = 0; I < nc; I++) lk.mptr[I + 1] += lk.mptr[I];
+        lk.mem.assign(F.n, 0);
+        {
+            std::vector<int> fill(lk.mptr.begin(), lk.mptr.end() - 1);
+            for (int i = 0; i < F.n; i++) lk.mem[fill[lk.agg[i]]++] = i;
+        }
+        HostLev C; C.n = nc; C.bptr.assign(nc + 1, 0);
+        std::vector<int> row;
+        for (int I = 0; I < nc; I++) {
+            row.clear();
+            for (int t = lk.mptr[I]; t < lk.mptr[I + 1]; t++) {
+                const int i = lk.mem[t];
+                for (int q = F.bptr[i]; q < F.bptr[i + 1]; q++) row.push_back(lk.agg[F.bcol[q]]);
+            }
+            std::sort(row.begin(), row.end());
+            row.erase(std::unique(row.begin(), row.end()), row.end());
+            C.bcol.insert(C.bcol.end(), row.begin(), row.end());
+            C.bptr[I + 1] = (int)C.bcol.size();
+        }
+        // Galerkin gather lists: fine block q (row i, column j) adds into coarse block (agg i, agg j)
+        const int nbf = F.bptr[F.n], nbc = (int)C.bcol.size();
+        std::vector<int> target(nbf);
+        lk.gptr.assign(nbc + 1, 0);
+        for (int i = 0; i < F.n; i++) {
+            const int I = lk.agg[i];
+            for (int q = F.bptr[i]; q < F.bptr[i + 1]; q++) {
+                const int J = lk.agg[F.bcol[q]];
+                const int t = (int)(std::lower_bound(C.bcol.begin() + C.bptr[I], C.bcol.begin() + C.bptr[I + 1], J) -
+                                    C.bcol.begin());
+                target[q] = t; lk.gptr[t + 1]++;
+            }
+        }
+        for (int t = 0; t < nbc; t++) lk.gptr[t + 1] += lk.gptr[t];
+        lk.gsrc.assign(nbf, 0);
+        {
+            std::vector<int> fill(lk.gptr.begin(), lk.gptr.end() - 1);
+            for (int q = 0; q < nbf; q++) lk.gsrc[fill[target[q]]++] = q;
+        }
+        K.push_back(std::move(lk));
+        L.push_back(std::move(C));
+    }
+    if (L.size() < 2) { g_err = "amg: the node graph cannot be coarsened"; return SW2G_ERR_MESH; }
+    for (size_t l = 1; l < L.size(); l++) {
+        HostLev& H = L[l];
+        H.dpos.assign(H.n, 0);
+        for (int i = 0; i < H.n; i++)
+            H.dpos[i] = (int)(std::lower_bound(H.bcol.begin() + H.bptr[i], H.bcol.begin() + H.bptr[i + 1], i) - H.bcol.begin());
+    }
+    auto up = [&](const int** dst, const std::vector<int>& v) {
+        int* d = nullptr;
+        int r = upload(m, &d, v.data(), v.size());
+        *dst = d;
+        return r;
+    };
+    AmgHost& A = m->amg;
+    A.nlev = (int)L.size();
+    for (int l = 0; l < A.nlev; l++) {
+        AmgLevel& D = A.lev[l];
+        const HostLev& H = L[l];
+        D.n = H.n;
+        const size_t n3 = 3 * (size_t)H.n;
+        TRY(dalloc(m, &D.b64, n3)); TRY(dalloc(m, &D.x64, n3)); TRY(dalloc(m, &D.t64, n3)); TRY(dalloc(m, &D.r64, n3));
+        TRY(dalloc(m, &D.b32, n3)); TRY(dalloc(m, &D.x32, n3)); TRY(dalloc(m, &D.t32, n3)); TRY(dalloc(m, &D.r32, n3));
+        if (l == 0) continue;   // level 0 is the reference CSR itself
+        D.nb = (int)H.bcol.size();
+        TRY(up(&D.bptr, H.bptr)); TRY(up(&D.bcol, H.bcol)); TRY(up(&D.dpos, H.dpos));
+        TRY(dalloc(m, &D.val64, 9 * (size_t)D.nb)); TRY(dalloc(m, &D.val32, 9 * (size_t)D.nb));
+        TRY(dalloc(m, &D.dinv64, 9 * (size_t)D.n)); TRY(dalloc(m, &D.dinv32, 9 * (size_t)D.n));
+    }
+    for (int l = 0; l + 1 < A.nlev; l++) {
+        AmgLink& D = A.link[l];
+        TRY(up(&D.agg, K[l].agg)); TRY(up(&D.mptr, K[l].mptr)); TRY(up(&D.mem, K[l].mem));
+        TRY(up(&D.gptr, K[l].gptr)); TRY(up(&D.gsrc, K[l].gsrc));
+    }
+    TRY(dalloc(m, &A.dinv0_64, 9 * (size_t)m->V)); TRY(dalloc(m, &A.dinv0_32, 9 * (size_t)m->V));
+    m->amg_ready = true;
+    static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;
+    if (trace) {
+        fprintf(stderr, "amg levels:");
+        for (auto& h : L) fprintf(stderr, " %d(%zu)", h.n, h.bcol.size());
+        fprintf(stderr, "\n");
+    }
+    return SW2G_OK;
+}
+
+// kernel launches of one preconditioner application (profiling counts)
+static int precond_launches(const sw2g_model* m, int precond) {
+    if (precond == SW2G_PC_BILU0) return 2 * m->ilu.ncolors;
+    if (precond == SW2G_PC_AMG) return 1 + (m->amg.nlev - 1) * (2 * kAmgNu + 4) + 1;
+    return 1;
+}
+
 template <class VT>
 static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_t* graph, int max_it, double atol,
                     double rtol, int* iters, int* status) {
     KrylovScalars init{};
     init.tol = atol; init.rtol = rtol; init.max_it = max_it;
     Reduce R{m->d_partial, m->d_counter, m->d_rout};
-    const bool ilu = precond == SW2G_PC_BILU0;
+    const bool pc = precond != SW2G_PC_BLOCK_JACOBI;
+    PrecondOp<VT> op;
+    op.kind = precond; op.ilu = &m->ilu; op.lu = V.vals_pc; op.dinv = V.inv; op.amg = &m->amg; op.vals = V.vals;
+    op.right = precond == SW2G_PC_AMG;
+    const int per_apply = precond == SW2G_PC_BILU0 ? 2 * m->ilu.ncolors : precond_launches(m, precond);
     {
-        ProfScope ps(m, 4, ilu ? 3 + 4 * m->ilu.ncolors : 2);
+        ProfScope ps(m, 4, pc ? 3 + 2 * per_apply : 2);
         CK(cudaMemcpyAsync(m->d_ks, &init, sizeof(KrylovScalars), cudaMemcpyHostToDevice, m->st));
-        if (ilu) launch_bicg_init_pc<VT>(m->B, m->ilu, V, m->d_ks, R, m->st);
+        if (pc) launch_bicg_init_pc<VT>(m->B, op, V, m->d_ks, R, m->st);
         else launch_bicg_init<VT>(m->B, V, m->d_ks, R, m->st);
         CKL();
     }
@@ -480,7 +639,7 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
         for (int c = 0; c < kChunk; c++) {
-            if (ilu) launch_bicg_iteration_pc<VT>(m->B, m->ilu, V, m->d_ks, R, m->st);
+            if (pc) launch_bicg_iteration_pc<VT>(m->B, op, V, m->d_ks, R, m->st);
             else launch_bicg_iteration<VT>(m->B, V, m->d_ks, R, m->st);
         }
         cudaError_t e1 = cudaGetLastError();
@@ -492,7 +651,7 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_
         CK(cudaGraphInstantiate(graph, g, 0));
         cudaGraphDestroy(g);
     }
-    const int per_it = ilu ? 6 + 4 * m->ilu.ncolors : 4;
+    const int per_it = pc ? 6 + 2 * per_apply : 4;
     static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;   // diagnostic: residual history on stderr
     while (true) {
         CK(cudaMemcpyAsync(m->h_ks, m->d_ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, m->st));
@@ -504,6 +663,11 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_
         ProfScope ps(m, 4, per_it * kChunk);
         CK(cudaGraphLaunch(*graph, m->st));
     }
+    if (op.right) {   // x holds y of A M^-1 y = b: x = M^-1 y
+        ProfScope ps(m, 4, per_apply);
+        precond_apply<VT>(m->B, op, V.x, nullptr, m->st);
+        CKL();
+    }
     *iters = m->h_ks->it;
     *status = m->h_ks->status;
     return SW2G_OK;
@@ -514,17 +678,190 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_
 // b is overwritten with M^-1 b as in the reference.
 static int solve64(sw2g_model* m, double* x, double* b, int precond, int max_it, double tol, int* iters, int* status) {
     CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * m->n, cudaMemcpyDeviceToDevice, m->st));
-    KrylovVecs<double> V{x, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, b, m->d_vals, m->d_inv, m->d_lu};
-    TRY(run_bicg<double>(m, V, precond, &m->graph64[precond == SW2G_PC_BILU0], max_it, tol, tol, iters, status));
+    KrylovVecs<double> V{x, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, b, m->d_vals, m->d_inv, m->d_lu, m->k_z};
+    TRY(run_bicg<double>(m, V, precond, &m->graph64[precond], max_it, tol, tol, iters, status));
     ProfScope ps(m, 5, 1);
     launch_unscale(m->n, m->d_x0, m->d_scale, x, m->st);
     CKL();
     return SW2G_OK;
 }
 
+// AMG path in FP64: right-preconditioned BiCGStab, restarted from the true FP64
+// residual after a breakdown or when the iteration budget of a pass ends, until
+// max|b - A x| <= tol + tol * max|b| on the scaled system.  A pass that does not
+// lower the residual is taken back and ends the solve (status 4).
+static int solve64_restarted(sw2g_model* m, double* x, double* b, int max_it, double tol, int max_restart, int* iters,
+                             int* passes, int* status) {
+    const int n = m->n;
+    Reduce R{m->d_partial, m->d_counter, m->d_rout};
+    CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_b64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemsetAsync(x, 0, sizeof(double) * n, m->st));
+    *iters = 0; *passes = 0; *status = 0;
+    double bn = -1, prev = 0;
+    for (int pass = 0;; pass++) {
+        {
+            ProfScope ps(m, 4, 2);
+            launch_spmv_sub(m->B, m->d_vals, x, m->d_b64, m->d_t64, m->st);
+            launch_maxabs(n, m->d_t64, R, m->st);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        const double rn = m->h_rout[0];
+        if (bn < 0) bn = rn;
+        if (!std::isfinite(rn)) { *status = 2; break; }
+        const double target = tol + tol * bn;
+        if (!(rn > target)) break;
+        if (pass > 0 && !(rn < prev)) {
+            ProfScope ps(m, 5, 1);
+            launch_axpy(n, -1.0, m->k_xi, x, m->st);
+            CKL();
+            if (!*status) *status = 4;
+            break;
+        }
+        if (pass > max_restart || *iters >= max_it) break;
+        prev = rn;
+        KrylovVecs<double> V{m->k_xi, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, m->d_t64, m->d_vals, m->d_inv,
+                             m->d_lu, m->k_z};
+        int it = 0, st = 0;
+        TRY(run_bicg<double>(m, V, SW2G_PC_AMG, &m->graph64[SW2G_PC_AMG], max_it - *iters, target, 0.0, &it, &st));
+        *iters += it; *passes += 1;
+        if (st == 2) { *status = 2; break; }
+        {
+            ProfScope ps(m, 5, 1);
+            launch_axpy(n, 1.0, m->k_xi, x, m->st);
+            CKL();
+        }
+    }
+    ProfScope ps(m, 5, 1);
+    launch_unscale(n, m->d_x0, m->d_scale, x, m->st);
+    CKL();
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ restarted GMRES
+static int alloc_gmres(sw2g_model* m, bool fp32) {
+    if (!m->gm.H) {
+        GmresDev& G = m->gm;
+        TRY(dalloc(m, &G.H, (size_t)kGmM * (kGmM + 1))); TRY(dalloc(m, &G.cs, kGmM)); TRY(dalloc(m, &G.sn, kGmM));
+        TRY(dalloc(m, &G.g, kGmM + 1)); TRY(dalloc(m, &G.y, kGmM));
+        TRY(dalloc(m, &G.partial, (size_t)kMaxBlocks * (kGmM + 1)));
+        TRY(dalloc(m, &G.counter, 1)); TRY(dalloc(m, &G.state, 4)); TRY(dalloc(m, &G.scal, 8));
+        CK(cudaMemsetAsync(G.counter, 0, sizeof(unsigned int), m->st));
+    }
+    if (!fp32 && !m->gm_V64) TRY(dalloc(m, &m->gm_V64, (size_t)(kGmM + 1) * m->n));
+    if (fp32 && !m->gm_V32) TRY(dalloc(m, &m->gm_V32, (size_t)(kGmM + 1) * m->n));
+    return SW2G_OK;
+}
+
+template <class VT>
+static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, VT* Vb, VT* z, const VT* rhs, VT* out, const VT* vals,
+                       const VT* lu, const VT* inv, int precond) {
+    if (*graph) return SW2G_OK;
+    PrecondOp<VT> op;
+    op.kind = precond; op.right = true; op.ilu = &m->ilu; op.lu = lu; op.dinv = inv; op.amg = &m->amg; op.vals = vals;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+    gmres_cycle<VT>(m->B, op, vals, Vb, (size_t)m->n, z, rhs, out, m->gm, m->st);
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        g_err = std::string("graph capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2);
+        return SW2G_ERR_CUDA;
+    }
+    CK(cudaGraphInstantiate(graph, g, 0));
+    cudaGraphDestroy(g);
+    return SW2G_OK;
+}
+
+// Restarted GMRES(kGmM) on the prepared (scaled) system: each pass forms the FP64
+// residual t = b - A x, runs one right-preconditioned cycle on it (FP64, or FP32
+// when `fp32`: matrix, preconditioner and basis in FP32) and adds the correction
+// in FP64.  Stops when max|t| <= tol + tol * max|b| (the reference's absolute +
+// relative form, on true residuals), after krylov_max_it inner iterations, or when
+// the residual stalls (three passes without a 1% decrease: status 4).  x keeps
+// the reference's x0 shift and unscaling.
+static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& o, bool fp32, int* iters,
+                       int* passes, int* status) {
+    const int n = m->n;
+    TRY(alloc_gmres(m, fp32));
+    if (fp32) TRY(alloc_fp32(m));
+    Reduce R{m->d_partial, m->d_counter, m->d_rout};
+    CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemcpyAsync(m->d_b64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+    CK(cudaMemsetAsync(x, 0, sizeof(double) * n, m->st));
+    if (fp32) {
+        ProfScope ps(m, 3, o.precond == SW2G_PC_BILU0 ? 3 : 2);
+        launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
+        launch_to_float(9 * m->V, m->d_inv, m->f_inv, m->st);
+        if (o.precond == SW2G_PC_BILU0) launch_to_float(m->nnz, m->d_lu, m->f_lu, m->st);
+        CKL();
+        TRY(gmres_graph<float>(m, &m->gm_graph32, m->gm_V32, m->f_z, m->f_b, m->f_x, m->f_vals, m->f_lu, m->f_inv,
+                               o.precond));
+    } else {
+        TRY(gmres_graph<double>(m, &m->gm_graph64, m->gm_V64, m->k_z, m->d_t64, m->k_xi, m->d_vals, m->d_lu, m->d_inv,
+                                o.precond));
+    }
+    const int per_cycle = kGmM * (6 + precond_launches(m, o.precond)) + 4 + precond_launches(m, o.precond);
+    *iters = 0; *passes = 0; *status = 0;
+    double bn = -1, prev = 0;
+    int stall = 0, cols = 0;
+    int hstate[4] = {0, 0, 0, 0};
+    for (int pass = 0;; pass++) {
+        {
+            ProfScope ps(m, 4, 2);
+            launch_spmv_sub(m->B, m->d_vals, x, m->d_b64, m->d_t64, m->st);
+            launch_maxabs(n, m->d_t64, R, m->st);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
+        if (pass > 0) CK(cudaMemcpyAsync(hstate, m->gm.state, sizeof(int) * 3, cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        if (pass > 0) {
+            cols = hstate[1]; *iters += cols;
+            if (hstate[2] == 2) { *status = 2; break; }
+        }
+        const double rn = m->h_rout[0];
+        if (bn < 0) bn = rn;
+        if (!std::isfinite(rn)) { *status = 2; break; }
+        const double target = o.krylov_tol + o.krylov_tol * bn;
+        if (!(rn > target)) break;
+        if (pass > 0) {
+            stall = (rn > 0.99 * prev) ? stall + 1 : 0;
+            if (stall >= 3) { *status = 4; break; }
+        }
+        if (*iters >= o.krylov_max_it) break;
+        prev = rn;
+        // one cycle aimed at the remaining reduction (2-norm estimate inside the cycle)
+        double rtol = target / rn;
+        if (fp32 && rtol < 1e-5) rtol = 1e-5;   // FP32 cannot resolve more in one cycle
+        CK(cudaMemcpyAsync(m->gm.scal + 3, &rtol, sizeof(double), cudaMemcpyHostToDevice, m->st));
+        {
+            ProfScope ps(m, 4, per_cycle + (fp32 ? 3 : 1));
+            if (fp32) {
+                launch_to_float(n, m->d_t64, m->f_b, m->st);
+                CK(cudaGraphLaunch(m->gm_graph32, m->st));
+                launch_to_double(n, m->f_x, m->d_t64 + n, m->st);
+                launch_axpy(n, 1.0, m->d_t64 + n, x, m->st);
+            } else {
+                CK(cudaGraphLaunch(m->gm_graph64, m->st));
+                launch_axpy(n, 1.0, m->k_xi, x, m->st);
+            }
+            CKL();
+        }
+        *passes += 1;
+    }
+    ProfScope ps(m, 5, 1);
+    launch_unscale(n, m->d_x0, m->d_scale, x, m->st);
+    CKL();
+    return SW2G_OK;
+}
+
 // FP32 BiCGStab inside FP64 iterative refinement, on the same scaled and
 // preconditioned system.  x accumulates in FP64.  Each pass forms the FP64
-// residual t = b - A x and applies the FP64 preconditioner; the reference's
+// residual t = b - A x and applies the FP64 preconditioner (left-preconditioned
+// kinds; the AMG path tests t itself); the reference's
 // stopping test (max|M^-1 t| <= tol + tol * max|M^-1 b|) ends the refinement;
 // otherwise A d = t is solved in FP32 (matrix, factor and vectors in FP32) to a
 // relative reduction refine_tol and d is added to x in FP64.
@@ -544,15 +881,22 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
         CKL();
     }
     *iters = 0; *passes = 0; *status = 0;
-    double bnorm = -1;
+    double bnorm = -1, prev_rn = 0;
     double* z = m->k_s;   // FP64 Krylov vectors are free in this mode
     for (int pass = 0; pass <= o.max_refine; pass++) {
         {
             ProfScope ps(m, 4, 3 + (ilu ? 2 * m->ilu.ncolors : 1));
             launch_spmv_sub(m->B, m->d_vals, x, m->d_b64, m->d_t64, m->st);
             CK(cudaMemcpyAsync(z, m->d_t64, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
-            if (ilu) launch_bilu_apply<double>(m->B, m->ilu, m->d_lu, m->d_inv, z, m->st);
-            else launch_bj_apply(m->V, m->d_inv, z, m->st);
+            if (o.precond == SW2G_PC_BLOCK_JACOBI) launch_bj_apply(m->V, m->d_inv, z, m->st);
+            else if (o.precond == SW2G_PC_AMG) {
+                // right-preconditioned inner solves: the test is on the true residual
+            } else {
+                PrecondOp<double> op;
+                op.kind = o.precond; op.ilu = &m->ilu; op.lu = m->d_lu; op.dinv = m->d_inv; op.amg = &m->amg;
+                op.vals = m->d_vals;
+                precond_apply<double>(m->B, op, z, nullptr, m->st);
+            }
             launch_maxabs(n, z, R, m->st);
             CKL();
         }
@@ -560,22 +904,31 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
         CK(cudaStreamSynchronize(m->st));
         const double rn = m->h_rout[0];
         if (bnorm < 0) bnorm = rn;                 // x = 0 on the first pass: M^-1 t = M^-1 b
+        if (pass > 0 && !(rn < prev_rn)) {         // the last FP32 correction did not help: take it back, stop
+            ProfScope ps(m, 5, 1);
+            launch_axpy(n, -1.0, m->d_t64 + n, x, m->st);
+            CKL();
+            if (!*status) *status = 4;
+            break;
+        }
         if (!std::isfinite(rn)) { *status = 2; break; }
         if (!(rn > o.krylov_tol + bnorm * o.krylov_tol) || pass == o.max_refine) break;
+        prev_rn = rn;
         {
             ProfScope ps(m, 4, 1);
             launch_to_float(n, m->d_t64, m->f_b, m->st);
             CKL();
         }
-        KrylovVecs<float> V32{m->f_x, m->f_r, m->f_p, m->f_Ap, m->f_q, m->f_s, m->f_As, m->f_b, m->f_vals, m->f_inv, m->f_lu};
+        KrylovVecs<float> V32{m->f_x, m->f_r, m->f_p, m->f_Ap, m->f_q, m->f_s, m->f_As, m->f_b, m->f_vals, m->f_inv, m->f_lu,
+                              m->f_z};
         int it = 0, st = 0;
-        TRY(run_bicg<float>(m, V32, o.precond, &m->graph32[ilu], o.krylov_max_it, 0.0, o.refine_tol, &it, &st));
+        TRY(run_bicg<float>(m, V32, o.precond, &m->graph32[o.precond], o.krylov_max_it, 0.0, o.refine_tol, &it, &st));
         *iters += it; *passes += 1;
         if (st == 1 || st == 2) *status = st;
         {
             ProfScope ps(m, 5, 2);
-            launch_to_double(n, m->f_x, m->d_t64, m->st);
-            launch_axpy(n, 1.0, m->d_t64, x, m->st);
+            launch_to_double(n, m->f_x, m->d_t64 + n, m->st);   // the correction, kept for a possible undo
+            launch_axpy(n, 1.0, m->d_t64 + n, x, m->st);
             CKL();
         }
         if (st == 2) break;
@@ -589,7 +942,17 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
 // ------------------------------------------------------------------ Newton step
 // fe_newton (src/newton/fe_newton.c:44-915), serial non-PETSc branch, on the
 // resident state d_sol / d_sol_old / d_sol_older / d_bc_mask / d_dirichlet.
+static bool valid_precond(int p) {
+    return p == SW2G_PC_BLOCK_JACOBI || p == SW2G_PC_BILU0 || p == SW2G_PC_AMG;
+}
 static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_stats* S) {
+    if (!(valid_precond(o.precond) && (o.krylov_precision == 32 || o.krylov_precision == 64) && o.krylov_max_it >= 0 &&
+          (o.krylov_method == SW2G_KRYLOV_BICGSTAB ||
+           (o.krylov_method == SW2G_KRYLOV_GMRES && o.precond != SW2G_PC_BLOCK_JACOBI)) &&
+          o.max_nonlin_it >= 0 && o.max_linesearch_cuts >= 0 && o.max_refine >= 0)) {
+        g_err = "sw2g newton: bad options";
+        return SW2G_ERR_ARG;
+    }
     const int n = m->n;
     sw2g_newton_stats st{};
     // initialize_system (newton_tools.c:21-53): sol <- sol_old, then fe_sw2_init:
@@ -615,15 +978,20 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
     TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
     if (!std::isfinite(rl2)) { g_err = "non-finite residual at the initial guess"; return SW2G_ERR_NONFINITE; }
     st.initial_resid_max = rmax;
-    int it = 0; bool ok = true, keep;
+    int it = 0; bool ok = true, keep, lin_stalled = false;
     do {
         TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
         CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
         TRY(do_prepare(m, m->d_vals, m->d_res, m->d_dsol));
         TRY(do_precond_setup(m, m->d_vals, o.precond));
         int kit = 0, kst = 0, passes = 0;
-        if (o.krylov_precision == 32) TRY(solve32(m, m->d_dsol, m->d_res, o, &kit, &passes, &kst));
+        if (o.krylov_method == SW2G_KRYLOV_GMRES)
+            TRY(solve_gmres(m, m->d_dsol, m->d_res, o, o.krylov_precision == 32, &kit, &passes, &kst));
+        else if (o.krylov_precision == 32) TRY(solve32(m, m->d_dsol, m->d_res, o, &kit, &passes, &kst));
+        else if (o.precond == SW2G_PC_AMG)
+            TRY(solve64_restarted(m, m->d_dsol, m->d_res, o.krylov_max_it, o.krylov_tol, o.max_refine, &kit, &passes, &kst));
         else TRY(solve64(m, m->d_dsol, m->d_res, o.precond, o.krylov_max_it, o.krylov_tol, &kit, &kst));
+        if (kst == 4) lin_stalled = true;
         st.krylov_its += kit; st.refine_passes += passes;
         if (kst == 1 || kst == 2) st.krylov_breakdowns++;
         {   // increment_function (newton_tools.c:261) and dsol = -dsol (fe_newton.c:553-555)
@@ -650,11 +1018,16 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
         }
         st.linesearch_cuts += cuts;
         it++;
+        static const bool trace = getenv("SW2G_TRACE_NEWTON") != nullptr;   // diagnostic: Newton history on stderr
+        if (trace)
+            fprintf(stderr, "newton it %d krylov %d status %d refine %d resid_max %.3e resid_l2 %.3e inc_max %.3e cuts %d\n",
+                    it, kit, kst, passes, rmax, rl2, imax, cuts);
         keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && imax > o.inc_nonlin;
     } while (keep);
     st.newton_its = it;
     st.resid_max = rmax; st.resid_l2 = rl2; st.inc_max = imax;
-    st.success = !((rmax > o.tol_nonlin && imax > o.inc_nonlin) || rmax >= 1.0E+20 || !ok);
+    // a linear solve that made no progress leaves a zero increment, which must not read as convergence
+    st.success = !((rmax > o.tol_nonlin && (imax > o.inc_nonlin || lin_stalled)) || rmax >= 1.0E+20 || !ok);
     if (!st.success) {   // fe_newton.c:887-890: reset to the old values
         CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
         launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
@@ -766,7 +1139,7 @@ extern "C" int sw2g_prepare_system(sw2g_model* m, double* vals, double* residual
 extern "C" int sw2g_solve_linear_sys_bcgstab(sw2g_model* m, double* x, const double* vals, double* b,
                                              const double* scale_vect, int max_it, double tol, int precond, int* iters) {
     NEED(m && x && vals && b && scale_vect && max_it >= 0 && tol >= 0 &&
-         (precond == SW2G_PC_BILU0 || precond == SW2G_PC_BLOCK_JACOBI), "sw2g_solve_linear_sys_bcgstab: bad argument");
+         valid_precond(precond), "sw2g_solve_linear_sys_bcgstab: bad argument");
     const size_t n = m->n;
     CK(cudaMemcpyAsync(m->d_vals, vals, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_res, b, sizeof(double) * n, cudaMemcpyHostToDevice, m->st));
@@ -851,5 +1224,43 @@ extern "C" int sw2g_reset_profile(sw2g_model* m) {
     NEED(m, "null model");
     prof_collect(m);
     for (int c = 0; c < SW2G_NCLASSES; c++) { m->prof_ms[c] = 0; m->prof_launch[c] = 0; }
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_ms, double* bytes) {
+    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 4, "sw2g_time_kernel: bad argument");
+    const double nnz = m->nnz, n = m->n, T = m->T, S = m->S;
+    if (which == 4) {
+        if (!m->amg_ready) TRY(build_amg(m));
+        amg_setup(m->B, m->amg, m->A, m->d_vals, m->st);
+    }
+    auto launch = [&]() {
+        switch (which) {
+            case 0: launch_spmv64(m->B, m->d_vals, m->k_p, m->k_Ap, m->st); break;
+            case 1: launch_elem_jac(m->M, m->P, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_wd, m->d_EJ, m->st); break;
+            case 2: launch_elem_resid(m->M, m->P, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_wd, m->d_ER, m->st); break;
+            case 3: launch_gather_jac(m->A, m->d_EJ, m->Etot, m->d_vals, m->st); break;
+            case 4: amg_smooth0_once(m->B, m->amg, m->d_vals, m->k_p, m->k_Ap, m->k_As, m->st); break;
+        }
+    };
+    launch();   // warm-up
+    CKL();
+    cudaEvent_t a = ev_get(m), b = ev_get(m);
+    CK(cudaEventRecord(a, m->st));
+    for (int r = 0; r < reps; r++) launch();
+    CK(cudaEventRecord(b, m->st));
+    CK(cudaEventSynchronize(b));
+    CKL();
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    m->ev_pool.push_back(a); m->ev_pool.push_back(b);
+    *avg_ms = ms / reps;
+    switch (which) {   // algorithmic bytes of one launch
+        case 0: *bytes = 12.0 * nnz + 20.0 * n; break;                      // CSR SpMV: vals+cols, rowptr+x+y
+        case 1: *bytes = 1290.0 * T + 632.0 * S; break;                     // element inputs + slot ids + 81/36 writes
+        case 2: *bytes = 316.0 * T + 200.0 * S + 8.0 * n; break;            // element inputs + residual out
+        case 3: *bytes = 8.0 * 81.0 * T + 8.0 * 36.0 * S + 12.0 * nnz; break;   // element blocks in, CSR values + map out
+        case 4: *bytes = 12.0 * nnz + 20.0 * n + 24.0 * n + 16.0 * n; break;    // SpMV + block-Jacobi apply
+    }
     return SW2G_OK;
 }

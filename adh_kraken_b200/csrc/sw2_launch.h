@@ -59,6 +59,7 @@ struct KrylovVecs {       // VT: double (FP64 path) or float (FP32 path)
     const VT* vals;       // matrix values in the reference CSR order
     const VT* inv;        // [nnodes*9] block-Jacobi inverses, or the inverted ILU diagonal blocks
     const VT* vals_pc;    // block-ILU factor in the CSR layout (unused by block-Jacobi)
+    VT* z;                // work vector of the right-preconditioned form (M^-1 p, M^-1 s)
 };
 
 template <class VT>
@@ -88,15 +89,107 @@ template <class VT>
 void launch_bilu_apply(const BlockCSR& A, const IluHost& H, const VT* lu, const VT* dinv, VT* y, cudaStream_t st);
 int grid_for_nodes(long nodes);   // grid for 8-lanes-per-node kernels
 
-// BiCGStab with an explicit preconditioner apply (block ILU): same scalars and
-// stopping rule as the fused block-Jacobi kernels above.
+// ---- aggregation AMG over the node blocks (amg_kernels.cu)
+constexpr int kAmgMaxLevels = 10;
+constexpr int kAmgNu = 2;               // block-Jacobi sweeps before and after each coarse correction
+constexpr double kAmgOmega = 0.67;      // damping of the sweeps
+constexpr double kAmgL1Theta = 0.1;     // l1 fix-up of a row: |a_vv| < theta * off-block row sum
+constexpr double kAmgGainMax = 20.0;    // l1 fix-up of a block: ||D^-1|| * off-block row sum above this
+constexpr int kAmgCoarseSweeps = 30;    // sweeps on the coarsest level
+constexpr int kAmgCoarsest = 256;       // stop coarsening at this many nodes
+struct AmgLevel {                       // device pointers; level 0 uses only the vector buffers
+    int n = 0, nb = 0;                  // rows (nodes) and 3x3 blocks
+    const int* bptr = nullptr;          // [n+1] block CSR
+    const int* bcol = nullptr;          // [nb]
+    const int* dpos = nullptr;          // [n] position of the diagonal block
+    double* val64 = nullptr; double* dinv64 = nullptr;   // [9*nb], [9*n]
+    float* val32 = nullptr; float* dinv32 = nullptr;
+    double *b64 = nullptr, *x64 = nullptr, *t64 = nullptr, *r64 = nullptr;   // [3n] each
+    float *b32 = nullptr, *x32 = nullptr, *t32 = nullptr, *r32 = nullptr;
+};
+struct AmgLink {                        // level l -> level l+1
+    const int* agg = nullptr;           // [n_l] aggregate of each node
+    const int* mptr = nullptr;          // [n_{l+1}+1] members of each aggregate, increasing node order
+    const int* mem = nullptr;
+    const int* gptr = nullptr;          // [nb_{l+1}+1] fine blocks summed into each coarse block
+    const int* gsrc = nullptr;          // level 0: slot ids of the node graph; else block ids
+};
+struct AmgHost {
+    int nlev = 0;                       // levels including level 0
+    AmgLevel lev[kAmgMaxLevels];
+    AmgLink link[kAmgMaxLevels];
+    double* dinv0_64 = nullptr; float* dinv0_32 = nullptr;   // [9*nnodes] level-0 smoother blocks
+};
+template <class VT> struct AmgBuf;
+template <> struct AmgBuf<double> {
+    static const double* val(const AmgLevel& L) { return L.val64; }
+    static const double* dinv(const AmgLevel& L) { return L.dinv64; }
+    static const double* dinv0(const AmgHost& H) { return H.dinv0_64; }
+    static double* b(const AmgLevel& L) { return L.b64; }
+    static double* x(const AmgLevel& L) { return L.x64; }
+    static double* t(const AmgLevel& L) { return L.t64; }
+    static double* r(const AmgLevel& L) { return L.r64; }
+};
+template <> struct AmgBuf<float> {
+    static const float* val(const AmgLevel& L) { return L.val32; }
+    static const float* dinv(const AmgLevel& L) { return L.dinv32; }
+    static const float* dinv0(const AmgHost& H) { return H.dinv0_32; }
+    static float* b(const AmgLevel& L) { return L.b32; }
+    static float* x(const AmgLevel& L) { return L.x32; }
+    static float* t(const AmgLevel& L) { return L.t32; }
+    static float* r(const AmgLevel& L) { return L.r32; }
+};
+// numeric set-up from the scaled level-0 matrix (FP64, plus FP32 copies)
+void amg_setup(const BlockCSR& A, const AmgHost& H, const AssemblyMaps& maps, const double* vals, cudaStream_t st);
+// one level-0 smoothing sweep y = x + w Dinv (b - A x) (FP64; kernel timing)
+void amg_smooth0_once(const BlockCSR& A, const AmgHost& H, const double* vals, const double* b, const double* x, double* y,
+                      cudaStream_t st);
+// y <- V-cycle(y); vals0 = the level-0 values in the Krylov precision
 template <class VT>
-void launch_bicg_init_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+void amg_apply(const BlockCSR& A, const AmgHost& H, const VT* vals0, VT* y, const int* skip, cudaStream_t st);
+
+// ---- preconditioner dispatch for the BiCGStab "_pc" path
+template <class VT>
+struct PrecondOp {
+    int kind = 0;                       // 1: block ILU(0), 2: aggregation AMG
+    bool right = false;                 // right preconditioning: BiCGStab on A M^-1 (true residuals)
+    const IluHost* ilu = nullptr; const VT* lu = nullptr; const VT* dinv = nullptr;
+    const AmgHost* amg = nullptr; const VT* vals = nullptr;
+};
+template <class VT>
+void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st);
+
+// ---- restarted GMRES(m) cycle (gmres_kernels.cu)
+constexpr int kGmM = 30;                // Krylov dimension of one cycle
+struct GmresDev {                       // device buffers of one cycle
+    double* H = nullptr;                // [kGmM][kGmM+1] Hessenberg columns (rotated in place)
+    double* cs = nullptr; double* sn = nullptr;   // [kGmM] Givens rotations
+    double* g = nullptr;                // [kGmM+1] rotated right-hand side
+    double* y = nullptr;                // [kGmM] least-squares solution
+    double* partial = nullptr;          // [kMaxBlocks*(kGmM+1)] block partials
+    unsigned int* counter = nullptr;    // last-block counter (wraps to 0)
+    int* state = nullptr;               // [0] done, [1] columns built, [2] status (0 ok, 1 breakdown, 2 non-finite)
+    double* scal = nullptr;             // [0] beta, [1] target, [2] residual estimate, [3] rtol (host-set), [4] h_{j+1,j}
+};
+// out = M^-1 V_k y from one cycle on rhs (x0 = 0); Vb holds kGmM+1 vectors of stride ld
+template <class VT>
+void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
+                 VT* out, const GmresDev& G, cudaStream_t st);
+template <class VT>
+void copy_skip(int n, const VT* a, VT* b, const int* skip, cudaStream_t st);
+template <class VT>
+void spmv_skip(const BlockCSR& A, const VT* vals, const VT* x, VT* y, const int* skip, cudaStream_t st);
+
+// BiCGStab with an explicit preconditioner apply: same scalars and stopping rule
+// as the fused block-Jacobi kernels above.
+template <class VT>
+void launch_bicg_init_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
                          cudaStream_t st);
 template <class VT>
-void launch_bicg_iteration_pc(const BlockCSR& A, const IluHost& H, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
+void launch_bicg_iteration_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
                               cudaStream_t st);
 
+void launch_spmv64(const BlockCSR& A, const double* vals, const double* x, double* y, cudaStream_t st);   // y = A x
 // FP64 refinement helpers: t = b - A x ; z <- M^-1 z (block-Jacobi) ; out[0] = max |z|
 void launch_spmv_sub(const BlockCSR& A, const double* vals, const double* x, const double* b, double* t, cudaStream_t st);
 void launch_bj_apply(int nnodes, const double* inv, double* z, cudaStream_t st);

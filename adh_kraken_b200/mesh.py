@@ -208,15 +208,17 @@ def basin_case(n: int = 707, seed: int = 2, nsteps: int = 200) -> SW2Case:
     return SW2Case("basin", xyz, tri, seg, kind, sol0, dt, nsteps, series)
 
 
-def beach_case(nx: int = 2828, ny: int = 707, seed: int = 3, nsteps: int = 300) -> SW2Case:
+def beach_case(nx: int = 2828, ny: int = 707, seed: int = 3, nsteps: int = 300, ly: float = 10000.0) -> SW2Case:
     """Wet/dry sloping beach: 40 km x 10 km jittered Delaunay (nx x ny; the default
     2828 x 707 gives ~4M triangles), bed rising linearly from -20 m (x = 0) to +3 m
     (x = 40 km) plus N(0, 0.2 m) noise, still water at eta = 0 so the upper beach is
     dry (h = eta - z <= 0, the reference's wet/dry convention), inflow hydrograph
     Q(t) = 500 + 1500 sin^2(pi t / 6 h) m^3/s imposed as the normal velocity
-    Q / (10 km * 20 m) on the deep edge, dt = 120 s."""
+    Q / (10 km * 20 m) on the deep edge, dt = 120 s.  `ly` < 10 km cuts a strip of
+    the same resolution (ny points across ly) that keeps the unit-width discharge,
+    i.e. the same inflow velocity."""
     rng = np.random.default_rng(seed)
-    LX, LY = 40000.0, 10000.0
+    LX, LY = 40000.0, float(ly)
     x, y, tri, (ii, jj) = jittered_delaunay(nx, ny, LX, LY, 0.3, rng)
     z = -20.0 + 23.0 * x / LX + rng.normal(0.0, 0.2, size=x.shape)
     west = np.arange(ny)
@@ -232,7 +234,7 @@ def beach_case(nx: int = 2828, ny: int = 707, seed: int = 3, nsteps: int = 300) 
     tf = dt * nsteps
     t = np.arange(0.0, tf + dt, dt / 4.0)
     q = 500.0 + 1500.0 * np.sin(np.pi * t / (6 * 3600.0)) ** 2
-    series = {0: _const_series(0.0, tf + dt, 20.0), 1: (t, q / (LY * 20.0)), 2: _const_series(0.0, tf + dt, 0.0)}
+    series = {0: _const_series(0.0, tf + dt, 20.0), 1: (t, q / (10000.0 * 20.0)), 2: _const_series(0.0, tf + dt, 0.0)}
     return SW2Case("beach", xyz, tri, seg, kind, sol0, dt, nsteps, series)
 
 

@@ -55,12 +55,21 @@ typedef struct {
     double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
     int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
     int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess instead of sol_old */
-    int precond;              /* SW2G_PC_BILU0 (default) or SW2G_PC_BLOCK_JACOBI */
+    int precond;              /* SW2G_PC_AMG (default), SW2G_PC_BILU0 or SW2G_PC_BLOCK_JACOBI */
+    int krylov_method;        /* SW2G_KRYLOV_GMRES (default; needs SW2G_PC_AMG or SW2G_PC_BILU0) or SW2G_KRYLOV_BICGSTAB */
 } sw2g_newton_opts;
+
+/* Krylov methods of the Newton correction.  BiCGStab is the reference's
+ * (bcgstab_solver.c:65-330).  GMRES(30), right-preconditioned and restarted from
+ * the true FP64 residual, is robust where an approximate preconditioner leaves a
+ * far-from-normal operator (BiCGStab's residual then swings or diverges). */
+#define SW2G_KRYLOV_BICGSTAB 0
+#define SW2G_KRYLOV_GMRES 1
 
 /* preconditioners standing in for the reference's full UMFPACK LU (bcgstab_solver.c:371-420) */
 #define SW2G_PC_BLOCK_JACOBI 0   /* 3x3 nodal block-Jacobi */
 #define SW2G_PC_BILU0 1          /* multicolour 3x3 block ILU(0) over the node graph */
+#define SW2G_PC_AMG 2            /* aggregation AMG V-cycle over the node blocks (l1 block-Jacobi smoothing) */
 
 typedef struct {
     int newton_its;           /* Newton iterations of the step */
@@ -148,6 +157,12 @@ void *sw2g_stream(sw2g_model *m);
 int sw2g_set_profiling(sw2g_model *m, int on);
 int sw2g_get_profile(sw2g_model *m, double *ms, long long *launches);
 int sw2g_reset_profile(sw2g_model *m);
+/* Times `reps` launches of one kernel on the resident data (CUDA events on the
+ * model's stream) and returns the mean launch time and the algorithmic bytes of
+ * one launch: 0 FP64 SpMV, 1 FD Jacobian element kernels, 2 element residual,
+ * 3 Jacobian gather, 4 AMG level-0 smoothing sweep.  Instrumentation for roofline
+ * reporting; no counterpart in the reference. */
+int sw2g_time_kernel(sw2g_model *m, int which, int reps, double *avg_ms, double *bytes);
 
 #ifdef __cplusplus
 }

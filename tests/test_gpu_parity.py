@@ -65,12 +65,16 @@ def test_dirichlet_and_scaling_bit_exact(name):
     assert np.array_equal(res, z["ref_residual_scaled"])
 
 
+PRECONDS = [0, 1, 2]   # block-Jacobi, block ILU(0), aggregation AMG
+
+
+@pytest.mark.parametrize("precond", PRECONDS)
 @pytest.mark.parametrize("name", DUMPS)
-def test_bicgstab_reaches_reference_solution(name):
+def test_bicgstab_reaches_reference_solution(name, precond):
     case, z = load(name)
     g, _ = gpu_model(case)
     x, b, it = g.bicgstab(z["ref_jac_vals_scaled"], z["ref_residual_scaled"], np.zeros(3 * case.nnodes),
-                          z["ref_scale_vect"], max_it=20000, tol=1e-13)
+                          z["ref_scale_vect"], max_it=20000, tol=1e-13, precond=precond)
     assert it > 0
     ref = z["ref_dsol"]
     # the two preconditioners reach the same solution to the conditioning of the system
@@ -89,12 +93,29 @@ def test_time_steps_match_reference(name):
     assert max(rel_err(sol, ref)) < 1e-8, rel_err(sol, ref)
 
 
+@pytest.mark.parametrize("krylov", [0, 1])   # BiCGStab, restarted GMRES
+@pytest.mark.parametrize("precond", [1, 2])
 @pytest.mark.parametrize("name", RUNS)
-def test_fp32_krylov_with_refinement_matches_reference(name):
+def test_time_steps_match_reference_each_solver(name, precond, krylov):
     from adh_kraken_b200.capi import default_opts
     from adh_kraken_b200.timeloop import SW2Simulation
     case, z = load(name)
-    sim = SW2Simulation(case, opts=default_opts(krylov_precision=32))
+    sim = SW2Simulation(case, opts=default_opts(precond=precond, krylov_method=krylov))
+    hist = sim.run(case.nsteps)
+    assert all(h["success"] for h in hist)
+    sol = sim.state()[0]
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
+    assert max(rel_err(sol, ref)) < 1e-8, rel_err(sol, ref)
+
+
+@pytest.mark.parametrize("krylov", [0, 1])
+@pytest.mark.parametrize("precond", [1, 2])
+@pytest.mark.parametrize("name", RUNS)
+def test_fp32_krylov_with_refinement_matches_reference(name, precond, krylov):
+    from adh_kraken_b200.capi import default_opts
+    from adh_kraken_b200.timeloop import SW2Simulation
+    case, z = load(name)
+    sim = SW2Simulation(case, opts=default_opts(krylov_precision=32, precond=precond, krylov_method=krylov))
     hist = sim.run(case.nsteps)
     assert all(h["success"] for h in hist)
     sol = sim.state()[0]
