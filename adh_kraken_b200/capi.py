@@ -36,7 +36,8 @@ class NewtonOpts(C.Structure):
     _fields_ = [("tol_nonlin", C.c_double), ("inc_nonlin", C.c_double), ("max_nonlin_it", C.c_int),
                 ("max_linesearch_cuts", C.c_int), ("krylov_max_it", C.c_int), ("krylov_tol", C.c_double),
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
-                ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int)]
+                ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int),
+                ("tol_nonlin_rel", C.c_double)]
 
 PC_BLOCK_JACOBI = 0
 PC_BILU0 = 1
@@ -49,7 +50,7 @@ class NewtonStats(C.Structure):
     _fields_ = [("newton_its", C.c_int), ("krylov_its", C.c_int), ("linesearch_cuts", C.c_int),
                 ("refine_passes", C.c_int), ("success", C.c_int), ("krylov_breakdowns", C.c_int),
                 ("resid_max", C.c_double), ("resid_l2", C.c_double), ("inc_max", C.c_double),
-                ("initial_resid_max", C.c_double)]
+                ("initial_resid_max", C.c_double), ("prev_resid_max", C.c_double), ("guess_used", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -243,7 +244,8 @@ class SW2Model:
 
     def time_kernel(self, which, reps=20):
         """(mean ms per launch, algorithmic bytes per launch) of kernel family `which`:
-        0 FP64 SpMV, 1 FD Jacobian, 2 element residual, 3 Jacobian gather, 4 AMG smoothing sweep."""
+        0 FP64 SpMV, 1 FD Jacobian, 2 element residual, 3 Jacobian gather, 4 AMG smoothing sweep (FP64),
+        5 AMG smoothing sweep (FP32)."""
         ms, by = C.c_double(), C.c_double()
         self._check(lib().sw2g_time_kernel(self.h, int(which), int(reps), C.byref(ms), C.byref(by)))
         return ms.value, by.value

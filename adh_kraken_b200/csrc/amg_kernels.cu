@@ -392,6 +392,11 @@ void amg_smooth0_once(const BlockCSR& A, const AmgHost& H, const double* vals, c
     k_amg_l0<double, 1><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, H.dinv0_64, b, x, y, kAmgOmega, nullptr);
 }
 
+void amg_smooth0_once32(const BlockCSR& A, const AmgHost& H, const float* vals, const float* b, const float* x, float* y,
+                        cudaStream_t st) {
+    k_amg_l0<float, 1><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, H.dinv0_32, b, x, y, kAmgOmega, nullptr);
+}
+
 template <class VT>
 void amg_apply(const BlockCSR& A, const AmgHost& H, const VT* vals0, VT* y, const int* skip, cudaStream_t st) {
     VT* b0 = AmgBuf<VT>::b(H.lev[0]);

@@ -9,9 +9,10 @@
 // cycle it serves both the FP64 solve and the FP32 inner solve of the iterative
 // refinement.
 //
-// A cycle from x = 0 on right-hand side r:
-//   beta = ||r||_2, v_0 = r / beta, g = beta e_0
-//   for j < m:  w = A M^-1 v_j ; h_{:,j} = V_j^T w (one multi-dot pass) ;
+// A cycle from x = 0 on right-hand side r, minimising ||W (r - A M^-1 V y)||_2 for
+// the row weights W = diag(rw):
+//   beta = ||W r||_2, v_0 = W r / beta, g = beta e_0
+//   for j < m:  w = W A M^-1 v_j ; h_{:,j} = V_j^T w (one multi-dot pass) ;
 //               w -= V_j h_{:,j} ; h_{j+1,j} = ||w|| ; v_{j+1} = w / h_{j+1,j} ;
 //               Givens rotation of column j ; stop when |g_{j+1}| <= rtol * beta
 //   y = H^-1 g (k x k triangular), out = M^-1 (V_k y)
@@ -51,11 +52,12 @@ __device__ __forceinline__ bool gm_last_block(const GmresDev& G) {
 
 // beta = ||r||_2 ; g = beta e_0 ; target = rtol * beta ; columns = 0
 template <class VT>
-__global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ r, GmresDev G) {
+__global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ r, const double* __restrict__ rw,
+                                                  GmresDev G) {
     __shared__ double sh[8];
     double ss = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double v = r[i];
+        const double v = (double)r[i] * rw[i];
         ss += v * v;
     }
 #pragma unroll
@@ -83,10 +85,18 @@ __global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ 
 }
 
 template <class VT>
-__global__ void k_gm_v0(int n, const VT* __restrict__ r, VT* __restrict__ v0, GmresDev G) {
+__global__ void k_gm_v0(int n, const VT* __restrict__ r, const double* __restrict__ rw, VT* __restrict__ v0, GmresDev G) {
     if (G.state[0]) return;
     const double inv = 1.0 / G.scal[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v0[i] = (VT)((double)r[i] * inv);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        v0[i] = (VT)((double)r[i] * rw[i] * inv);
+}
+
+// w <- rw o w (row weights of the minimised residual norm)
+template <class VT>
+__global__ void k_gm_rowweight(int n, VT* __restrict__ w, const double* __restrict__ rw, GmresDev G) {
+    if (G.state[0]) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = (VT)((double)w[i] * rw[i]);
 }
 
 // h_k = v_k . w for k < nv (w = v_nv before orthogonalisation), into column j of H
@@ -218,17 +228,18 @@ __global__ void k_gm_combine(int n, const VT* __restrict__ Vb, size_t ld, VT* __
 
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const GmresDev& G, cudaStream_t st) {
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st) {
     const int n = A.n, g = gm_grid(n);
     const int* done = G.state;
-    k_gm_start<VT><<<g, 256, 0, st>>>(n, rhs, G);
-    k_gm_v0<VT><<<g, 256, 0, st>>>(n, rhs, Vb, G);
+    k_gm_start<VT><<<g, 256, 0, st>>>(n, rhs, rw, G);
+    k_gm_v0<VT><<<g, 256, 0, st>>>(n, rhs, rw, Vb, G);
     for (int j = 0; j < kGmM; j++) {
         VT* vj = Vb + (size_t)j * ld;
         VT* w = Vb + (size_t)(j + 1) * ld;
         copy_skip<VT>(n, vj, z, done, st);
         precond_apply<VT>(A, P, z, done, st);
         spmv_skip<VT>(A, vals, z, w, done, st);
+        k_gm_rowweight<VT><<<g, 256, 0, st>>>(n, w, rw, G);
         k_gm_dots<VT><<<g, 256, 0, st>>>(n, j + 1, Vb, ld, j, G);
         k_gm_orth<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
         k_gm_scale<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
@@ -238,8 +249,8 @@ void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* 
     precond_apply<VT>(A, P, out, nullptr, st);
 }
 template void gmres_cycle<double>(const BlockCSR&, const PrecondOp<double>&, const double*, double*, size_t, double*,
-                                  const double*, double*, const GmresDev&, cudaStream_t);
+                                  const double*, double*, const double*, const GmresDev&, cudaStream_t);
 template void gmres_cycle<float>(const BlockCSR&, const PrecondOp<float>&, const float*, float*, size_t, float*,
-                                 const float*, float*, const GmresDev&, cudaStream_t);
+                                 const float*, float*, const double*, const GmresDev&, cudaStream_t);
 
 }  // namespace sw2

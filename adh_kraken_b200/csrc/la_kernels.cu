@@ -650,7 +650,27 @@ void launch_spmv64(const BlockCSR& A, const double* vals, const double* x, doubl
 }
 
 template <class VT>
+__global__ void k_cast_skip(int n, const VT* __restrict__ a, float* __restrict__ b, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+template <class VT>
+__global__ void k_uncast_skip(int n, const float* __restrict__ a, VT* __restrict__ b, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (VT)a[i];
+}
+
+template <class VT>
 void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st) {
+    if (P.mixed) {
+        PrecondOp<float> P32;
+        P32.kind = P.kind; P32.ilu = P.ilu; P32.lu = P.lu32; P32.dinv = P.dinv32; P32.amg = P.amg; P32.vals = P.vals32;
+        const int g = grid_for(A.n, 256);
+        k_cast_skip<VT><<<g, 256, 0, st>>>(A.n, y, P.tmp32, skip);
+        precond_apply<float>(A, P32, P.tmp32, skip, st);
+        k_uncast_skip<VT><<<g, 256, 0, st>>>(A.n, P.tmp32, y, skip);
+        return;
+    }
     if (P.kind == 2) {
         amg_apply<VT>(A, *P.amg, P.vals, y, skip, st);
     } else {
@@ -797,6 +817,31 @@ __global__ void __launch_bounds__(256) k_maxabs(int n, const double* __restrict_
         for (int k = 0; k < (int)gridDim.x; k++) { a = fmax(a, ld_part(R, 4 * k)); b = fmax(b, ld_part(R, 4 * k + 1)); }
         R.out[0] = b > 0 ? NAN : a;   // a non-finite entry is reported, not hidden by fmax
     }
+}
+__global__ void __launch_bounds__(256) k_maxabs_unscaled(int n, const double* __restrict__ t, const double* __restrict__ sc,
+                                                         Reduce R) {
+    __shared__ double sh[8];
+    double m = 0, bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = fabs(t[i] / sc[i]);
+        if (!isfinite(a)) bad = 1; else m = fmax(m, a);
+    }
+    double v[2];
+    v[0] = block_max<256>(m, sh); v[1] = block_max<256>(bad, sh);
+    if (last_block(R, v, 2)) {
+        double a = 0, b = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) { a = fmax(a, ld_part(R, 4 * k)); b = fmax(b, ld_part(R, 4 * k + 1)); }
+        R.out[0] = b > 0 ? NAN : a;
+    }
+}
+__global__ void k_inv_scale(int n, const double* __restrict__ s, double* __restrict__ rw) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rw[i] = 1.0 / s[i];
+}
+void launch_inv_scale(int n, const double* scale, double* rw, cudaStream_t st) {
+    k_inv_scale<<<grid_for(n, 256), 256, 0, st>>>(n, scale, rw);
+}
+void launch_maxabs_unscaled(int n, const double* t, const double* scale, Reduce R, cudaStream_t st) {
+    k_maxabs_unscaled<<<grid_for(n, 256), 256, 0, st>>>(n, t, scale, R);
 }
 void launch_maxabs(int n, const double* z, Reduce R, cudaStream_t st) {
     k_maxabs<<<grid_for(n, 256), 256, 0, st>>>(n, z, R);

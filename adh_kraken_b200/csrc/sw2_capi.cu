@@ -85,7 +85,8 @@ struct sw2g_model {
     bool amg_ready = false;
     // restarted GMRES (allocated on first use)
     GmresDev gm{};
-    double* gm_V64 = nullptr; float* gm_V32 = nullptr;
+    double* gm_V64 = nullptr;            // [kGmM+1][n] Krylov basis
+    double* gm_rw = nullptr;             // [n] row weights 1/s: GMRES minimises the unscaled residual
     cudaGraphExec_t gm_graph64 = nullptr, gm_graph32 = nullptr;
     std::vector<int> h_bptr, h_bcol;   // node graph, kept for the AMG set-up
     StepParams P{};
@@ -174,6 +175,7 @@ extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->krylov_max_it = 4000; o->krylov_tol = 1e-11; o->krylov_precision = 64;
     o->refine_tol = 1e-4; o->max_refine = 8; o->use_guess = 0; o->precond = SW2G_PC_AMG;
     o->krylov_method = SW2G_KRYLOV_GMRES;
+    o->tol_nonlin_rel = 0.0;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -741,7 +743,7 @@ static int solve64_restarted(sw2g_model* m, double* x, double* b, int max_it, do
 }
 
 // ------------------------------------------------------------------ restarted GMRES
-static int alloc_gmres(sw2g_model* m, bool fp32) {
+static int alloc_gmres(sw2g_model* m) {
     if (!m->gm.H) {
         GmresDev& G = m->gm;
         TRY(dalloc(m, &G.H, (size_t)kGmM * (kGmM + 1))); TRY(dalloc(m, &G.cs, kGmM)); TRY(dalloc(m, &G.sn, kGmM));
@@ -750,20 +752,21 @@ static int alloc_gmres(sw2g_model* m, bool fp32) {
         TRY(dalloc(m, &G.counter, 1)); TRY(dalloc(m, &G.state, 4)); TRY(dalloc(m, &G.scal, 8));
         CK(cudaMemsetAsync(G.counter, 0, sizeof(unsigned int), m->st));
     }
-    if (!fp32 && !m->gm_V64) TRY(dalloc(m, &m->gm_V64, (size_t)(kGmM + 1) * m->n));
-    if (fp32 && !m->gm_V32) TRY(dalloc(m, &m->gm_V32, (size_t)(kGmM + 1) * m->n));
+    if (!m->gm_V64) TRY(dalloc(m, &m->gm_V64, (size_t)(kGmM + 1) * m->n));
+    if (!m->gm_rw) TRY(dalloc(m, &m->gm_rw, (size_t)m->n));
     return SW2G_OK;
 }
 
-template <class VT>
-static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, VT* Vb, VT* z, const VT* rhs, VT* out, const VT* vals,
-                       const VT* lu, const VT* inv, int precond) {
+static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, bool mixed, int precond) {
     if (*graph) return SW2G_OK;
-    PrecondOp<VT> op;
-    op.kind = precond; op.right = true; op.ilu = &m->ilu; op.lu = lu; op.dinv = inv; op.amg = &m->amg; op.vals = vals;
+    PrecondOp<double> op;
+    op.kind = precond; op.right = true; op.ilu = &m->ilu; op.lu = m->d_lu; op.dinv = m->d_inv; op.amg = &m->amg;
+    op.vals = m->d_vals;
+    if (mixed) { op.mixed = true; op.vals32 = m->f_vals; op.lu32 = m->f_lu; op.dinv32 = m->f_inv; op.tmp32 = m->f_z; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-    gmres_cycle<VT>(m->B, op, vals, Vb, (size_t)m->n, z, rhs, out, m->gm, m->st);
+    gmres_cycle<double>(m->B, op, m->d_vals, m->gm_V64, (size_t)m->n, m->k_z, m->d_t64, m->k_xi, m->gm_rw, m->gm,
+                        m->st);
     cudaError_t e1 = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
@@ -775,57 +778,64 @@ static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, VT* Vb, VT* z, con
     return SW2G_OK;
 }
 
-// Restarted GMRES(kGmM) on the prepared (scaled) system: each pass forms the FP64
-// residual t = b - A x, runs one right-preconditioned cycle on it (FP64, or FP32
-// when `fp32`: matrix, preconditioner and basis in FP32) and adds the correction
-// in FP64.  Stops when max|t| <= tol + tol * max|b| (the reference's absolute +
-// relative form, on true residuals), after krylov_max_it inner iterations, or when
-// the residual stalls (three passes without a 1% decrease: status 4).  x keeps
-// the reference's x0 shift and unscaling.
-static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& o, bool fp32, int* iters,
-                       int* passes, int* status) {
+// Restarted GMRES(kGmM) on the prepared (scaled) system, FP64 Krylov basis.  Each
+// pass forms the FP64 residual t = b - A x, runs one right-preconditioned cycle
+// on it and adds the correction.  The cycle minimises the 2-norm of the UNSCALED
+// residual S^-1 t (row weights 1/s), the quantity the Newton test looks at; the
+// symmetric scaling still conditions the operator and the AMG hierarchy.  With `mixed` the preconditioner runs in FP32
+// (FP32 matrix values, block inverses and AMG hierarchy on a rounded copy of the
+// vector): half the bytes of the dominant kernels, while the Krylov recurrence
+// and the residuals stay FP64, so the attainable accuracy is the FP64 one.
+// Stopping is inexact-Newton style on the UNSCALED linear residual r = S^-1 t:
+// max|r| <= max(krylov_tol * fnorm, 0.5 * tol_nonlin), with fnorm the current
+// Newton residual max-norm, so the Newton loop can reach tol_nonlin on the
+// reference's unscaled residual.  Also stops after krylov_max_it inner iterations
+// or when three passes in a row lower max|r| by less than 1% (status 4).
+static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& o, bool mixed, double fnorm,
+                       int* iters, int* passes, int* status) {
     const int n = m->n;
-    TRY(alloc_gmres(m, fp32));
-    if (fp32) TRY(alloc_fp32(m));
+    TRY(alloc_gmres(m));
+    if (mixed) TRY(alloc_fp32(m));
     Reduce R{m->d_partial, m->d_counter, m->d_rout};
     CK(cudaMemcpyAsync(m->d_x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_b64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
     CK(cudaMemsetAsync(x, 0, sizeof(double) * n, m->st));
-    if (fp32) {
+    if (mixed) {
         ProfScope ps(m, 3, o.precond == SW2G_PC_BILU0 ? 3 : 2);
         launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
         launch_to_float(9 * m->V, m->d_inv, m->f_inv, m->st);
         if (o.precond == SW2G_PC_BILU0) launch_to_float(m->nnz, m->d_lu, m->f_lu, m->st);
         CKL();
-        TRY(gmres_graph<float>(m, &m->gm_graph32, m->gm_V32, m->f_z, m->f_b, m->f_x, m->f_vals, m->f_lu, m->f_inv,
-                               o.precond));
-    } else {
-        TRY(gmres_graph<double>(m, &m->gm_graph64, m->gm_V64, m->k_z, m->d_t64, m->k_xi, m->d_vals, m->d_lu, m->d_inv,
-                                o.precond));
     }
-    const int per_cycle = kGmM * (6 + precond_launches(m, o.precond)) + 4 + precond_launches(m, o.precond);
+    {
+        ProfScope ps(m, 4, 1);
+        launch_inv_scale(n, m->d_scale, m->gm_rw, m->st);
+        CKL();
+    }
+    TRY(gmres_graph(m, mixed ? &m->gm_graph32 : &m->gm_graph64, mixed, o.precond));
+    const int pl = precond_launches(m, o.precond) + (mixed ? 2 : 0);
+    const int per_cycle = kGmM * (6 + pl) + 4 + pl;
+    const double target = std::max(o.krylov_tol * fnorm, 0.5 * o.tol_nonlin);
     *iters = 0; *passes = 0; *status = 0;
-    double bn = -1, prev = 0;
-    int stall = 0, cols = 0;
+    double prev = 0;
+    int stall = 0;
     int hstate[4] = {0, 0, 0, 0};
     for (int pass = 0;; pass++) {
         {
             ProfScope ps(m, 4, 2);
             launch_spmv_sub(m->B, m->d_vals, x, m->d_b64, m->d_t64, m->st);
-            launch_maxabs(n, m->d_t64, R, m->st);
+            launch_maxabs_unscaled(n, m->d_t64, m->d_scale, R, m->st);
             CKL();
         }
         CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
         if (pass > 0) CK(cudaMemcpyAsync(hstate, m->gm.state, sizeof(int) * 3, cudaMemcpyDeviceToHost, m->st));
         CK(cudaStreamSynchronize(m->st));
         if (pass > 0) {
-            cols = hstate[1]; *iters += cols;
+            *iters += hstate[1];
             if (hstate[2] == 2) { *status = 2; break; }
         }
         const double rn = m->h_rout[0];
-        if (bn < 0) bn = rn;
         if (!std::isfinite(rn)) { *status = 2; break; }
-        const double target = o.krylov_tol + o.krylov_tol * bn;
         if (!(rn > target)) break;
         if (pass > 0) {
             stall = (rn > 0.99 * prev) ? stall + 1 : 0;
@@ -833,21 +843,13 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         }
         if (*iters >= o.krylov_max_it) break;
         prev = rn;
-        // one cycle aimed at the remaining reduction (2-norm estimate inside the cycle)
-        double rtol = target / rn;
-        if (fp32 && rtol < 1e-5) rtol = 1e-5;   // FP32 cannot resolve more in one cycle
+        double rtol = 0.5 * target / rn;         // the cycle's own 2-norm estimate of the reduction still needed
+        if (rtol < 1e-12) rtol = 1e-12;
         CK(cudaMemcpyAsync(m->gm.scal + 3, &rtol, sizeof(double), cudaMemcpyHostToDevice, m->st));
         {
-            ProfScope ps(m, 4, per_cycle + (fp32 ? 3 : 1));
-            if (fp32) {
-                launch_to_float(n, m->d_t64, m->f_b, m->st);
-                CK(cudaGraphLaunch(m->gm_graph32, m->st));
-                launch_to_double(n, m->f_x, m->d_t64 + n, m->st);
-                launch_axpy(n, 1.0, m->d_t64 + n, x, m->st);
-            } else {
-                CK(cudaGraphLaunch(m->gm_graph64, m->st));
-                launch_axpy(n, 1.0, m->k_xi, x, m->st);
-            }
+            ProfScope ps(m, 4, per_cycle + 1);
+            CK(cudaGraphLaunch(mixed ? m->gm_graph32 : m->gm_graph64, m->st));
+            launch_axpy(n, 1.0, m->k_xi, x, m->st);
             CKL();
         }
         *passes += 1;
@@ -945,11 +947,11 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
 static bool valid_precond(int p) {
     return p == SW2G_PC_BLOCK_JACOBI || p == SW2G_PC_BILU0 || p == SW2G_PC_AMG;
 }
-static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_stats* S) {
-    if (!(valid_precond(o.precond) && (o.krylov_precision == 32 || o.krylov_precision == 64) && o.krylov_max_it >= 0 &&
-          (o.krylov_method == SW2G_KRYLOV_BICGSTAB ||
-           (o.krylov_method == SW2G_KRYLOV_GMRES && o.precond != SW2G_PC_BLOCK_JACOBI)) &&
-          o.max_nonlin_it >= 0 && o.max_linesearch_cuts >= 0 && o.max_refine >= 0)) {
+static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newton_stats* S) {
+    if (!(valid_precond(o_in.precond) && (o_in.krylov_precision == 32 || o_in.krylov_precision == 64) && o_in.krylov_max_it >= 0 &&
+          (o_in.krylov_method == SW2G_KRYLOV_BICGSTAB ||
+           (o_in.krylov_method == SW2G_KRYLOV_GMRES && o_in.precond != SW2G_PC_BLOCK_JACOBI)) &&
+          o_in.max_nonlin_it >= 0 && o_in.max_linesearch_cuts >= 0 && o_in.max_refine >= 0)) {
         g_err = "sw2g newton: bad options";
         return SW2G_ERR_ARG;
     }
@@ -964,9 +966,6 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
         launch_dry_mask(m->V, m->d_sol_old, m->d_bc_mask, m->st);
         CKL();
     }
-    // initial-guess hook: after initialize_system, before initialize_dirichlet_bc
-    if (o.use_guess && m->guess_set)
-        CK(cudaMemcpyAsync(m->d_sol, m->d_guess, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
     {   // initialize_dirichlet_bc (newton_tools.c:130)
         ProfScope ps(m, 5, 1);
         launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
@@ -977,7 +976,37 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
     TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
     TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
     if (!std::isfinite(rl2)) { g_err = "non-finite residual at the initial guess"; return SW2G_ERR_NONFINITE; }
+    st.prev_resid_max = rmax;
+    // Initial-guess hook (after initialize_system): a supplied guess replaces the
+    // previous-step state only if its residual max-norm is smaller -- the Newton
+    // residual judges the guess, the previous step is the fallback.
+    if (o_in.use_guess && m->guess_set) {
+        CK(cudaMemcpyAsync(m->d_sol, m->d_guess, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+        {
+            ProfScope ps(m, 5, 1);
+            launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
+            CKL();
+        }
+        double gmax, gl2, gi;
+        TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+        TRY(do_norms(m, m->d_res, m->d_dsol, &gmax, &gl2, &gi));
+        if (std::isfinite(gl2) && gmax < rmax) {
+            rmax = gmax; rl2 = gl2; imax = gi; st.guess_used = 1;
+        } else {   // fall back to the previous-step state
+            CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
+            {
+                ProfScope ps(m, 5, 1);
+                launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
+                CKL();
+            }
+            TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+            TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
+        }
+    }
     st.initial_resid_max = rmax;
+    sw2g_newton_opts o = o_in;   // the step's effective options
+    // relative test: against the previous-step state's residual, the same reference with or without a guess
+    if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = o_in.tol_nonlin_rel * st.prev_resid_max;
     int it = 0; bool ok = true, keep, lin_stalled = false;
     do {
         TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
@@ -986,12 +1015,12 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
         TRY(do_precond_setup(m, m->d_vals, o.precond));
         int kit = 0, kst = 0, passes = 0;
         if (o.krylov_method == SW2G_KRYLOV_GMRES)
-            TRY(solve_gmres(m, m->d_dsol, m->d_res, o, o.krylov_precision == 32, &kit, &passes, &kst));
+            TRY(solve_gmres(m, m->d_dsol, m->d_res, o, o.krylov_precision == 32, rmax, &kit, &passes, &kst));
         else if (o.krylov_precision == 32) TRY(solve32(m, m->d_dsol, m->d_res, o, &kit, &passes, &kst));
         else if (o.precond == SW2G_PC_AMG)
             TRY(solve64_restarted(m, m->d_dsol, m->d_res, o.krylov_max_it, o.krylov_tol, o.max_refine, &kit, &passes, &kst));
         else TRY(solve64(m, m->d_dsol, m->d_res, o.precond, o.krylov_max_it, o.krylov_tol, &kit, &kst));
-        if (kst == 4) lin_stalled = true;
+        const int lin_status = kst;
         st.krylov_its += kit; st.refine_passes += passes;
         if (kst == 1 || kst == 2) st.krylov_breakdowns++;
         {   // increment_function (newton_tools.c:261) and dsol = -dsol (fe_newton.c:553-555)
@@ -1003,9 +1032,10 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
         const double old_l2 = rl2;
         TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
         TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
-        if (std::isnan(rl2) || std::isinf(rl2)) ok = false;
         int cuts = 0;   // line search, fe_newton.c:681-741
-        while (rmax > o.tol_nonlin && rl2 > old_l2 && cuts < o.max_linesearch_cuts) {
+        // a step into a state whose residual is not finite (e.g. a depth driven below zero under the
+        // square root of the SUPG scale) is cut like a step that raised the residual
+        while (rmax > o.tol_nonlin && (rl2 > old_l2 || !std::isfinite(rl2)) && cuts < o.max_linesearch_cuts) {
             {
                 ProfScope ps(m, 5, 2);
                 launch_scal(n, 0.5, m->d_dsol, m->st);
@@ -1016,6 +1046,9 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_s
             TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
             cuts++;
         }
+        if (std::isnan(rl2) || std::isinf(rl2)) ok = false;
+        // a failed linear solve that left a zero increment must not read as an increment below inc_nonlin
+        lin_stalled = (lin_status != 0 && !(imax > 0.0));
         st.linesearch_cuts += cuts;
         it++;
         static const bool trace = getenv("SW2G_TRACE_NEWTON") != nullptr;   // diagnostic: Newton history on stderr
@@ -1228,11 +1261,15 @@ extern "C" int sw2g_reset_profile(sw2g_model* m) {
 }
 
 extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_ms, double* bytes) {
-    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 4, "sw2g_time_kernel: bad argument");
+    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 5, "sw2g_time_kernel: bad argument");
     const double nnz = m->nnz, n = m->n, T = m->T, S = m->S;
-    if (which == 4) {
+    if (which >= 4) {
         if (!m->amg_ready) TRY(build_amg(m));
         amg_setup(m->B, m->amg, m->A, m->d_vals, m->st);
+    }
+    if (which == 5) {
+        TRY(alloc_fp32(m));
+        launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
     }
     auto launch = [&]() {
         switch (which) {
@@ -1241,6 +1278,7 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
             case 2: launch_elem_resid(m->M, m->P, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_wd, m->d_ER, m->st); break;
             case 3: launch_gather_jac(m->A, m->d_EJ, m->Etot, m->d_vals, m->st); break;
             case 4: amg_smooth0_once(m->B, m->amg, m->d_vals, m->k_p, m->k_Ap, m->k_As, m->st); break;
+            case 5: amg_smooth0_once32(m->B, m->amg, m->f_vals, m->f_p, m->f_Ap, m->f_As, m->st); break;
         }
     };
     launch();   // warm-up
@@ -1261,6 +1299,7 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
         case 2: *bytes = 316.0 * T + 200.0 * S + 8.0 * n; break;            // element inputs + residual out
         case 3: *bytes = 8.0 * 81.0 * T + 8.0 * 36.0 * S + 12.0 * nnz; break;   // element blocks in, CSR values + map out
         case 4: *bytes = 12.0 * nnz + 20.0 * n + 24.0 * n + 16.0 * n; break;    // SpMV + block-Jacobi apply
+        case 5: *bytes = 8.0 * nnz + 12.0 * n + 12.0 * n + 8.0 * n; break;      // FP32-value SpMV + FP32 block apply
     }
     return SW2G_OK;
 }

@@ -144,6 +144,8 @@ void amg_setup(const BlockCSR& A, const AmgHost& H, const AssemblyMaps& maps, co
 // one level-0 smoothing sweep y = x + w Dinv (b - A x) (FP64; kernel timing)
 void amg_smooth0_once(const BlockCSR& A, const AmgHost& H, const double* vals, const double* b, const double* x, double* y,
                       cudaStream_t st);
+void amg_smooth0_once32(const BlockCSR& A, const AmgHost& H, const float* vals, const float* b, const float* x, float* y,
+                        cudaStream_t st);
 // y <- V-cycle(y); vals0 = the level-0 values in the Krylov precision
 template <class VT>
 void amg_apply(const BlockCSR& A, const AmgHost& H, const VT* vals0, VT* y, const int* skip, cudaStream_t st);
@@ -155,6 +157,11 @@ struct PrecondOp {
     bool right = false;                 // right preconditioning: BiCGStab on A M^-1 (true residuals)
     const IluHost* ilu = nullptr; const VT* lu = nullptr; const VT* dinv = nullptr;
     const AmgHost* amg = nullptr; const VT* vals = nullptr;
+    // mixed precision (VT = double only): apply the preconditioner in FP32 on a
+    // rounded copy of the vector, from the FP32 matrix / factor / AMG values
+    bool mixed = false;
+    const float* vals32 = nullptr; const float* lu32 = nullptr; const float* dinv32 = nullptr;
+    float* tmp32 = nullptr;             // [n] work vector
 };
 template <class VT>
 void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st);
@@ -171,12 +178,17 @@ struct GmresDev {                       // device buffers of one cycle
     int* state = nullptr;               // [0] done, [1] columns built, [2] status (0 ok, 1 breakdown, 2 non-finite)
     double* scal = nullptr;             // [0] beta, [1] target, [2] residual estimate, [3] rtol (host-set), [4] h_{j+1,j}
 };
-// out = M^-1 V_k y from one cycle on rhs (x0 = 0); Vb holds kGmM+1 vectors of stride ld
+// out = M^-1 V_k y from one cycle on rhs (x0 = 0), minimising the rw-weighted
+// residual 2-norm; Vb holds kGmM+1 vectors of stride ld
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const GmresDev& G, cudaStream_t st);
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st);
+// rw_i = 1 / s_i (weights that make a scaled system's residual the unscaled one)
+void launch_inv_scale(int n, const double* scale, double* rw, cudaStream_t st);
 template <class VT>
 void copy_skip(int n, const VT* a, VT* b, const int* skip, cudaStream_t st);
+// max_i |t_i / s_i|: the unscaled residual of a scaled system (out[0] of R)
+void launch_maxabs_unscaled(int n, const double* t, const double* scale, Reduce R, cudaStream_t st);
 template <class VT>
 void spmv_skip(const BlockCSR& A, const VT* vals, const VT* x, VT* y, const int* skip, cudaStream_t st);
 

@@ -54,9 +54,13 @@ typedef struct {
     int krylov_precision;     /* 64: FP64 BiCGStab; 32: FP32 BiCGStab inside FP64 iterative refinement */
     double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
     int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
-    int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess instead of sol_old */
+    int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess when its residual
+                                 max-norm is below that of sol_old (else sol_old, the reference's start) */
     int precond;              /* SW2G_PC_AMG (default), SW2G_PC_BILU0 or SW2G_PC_BLOCK_JACOBI */
     int krylov_method;        /* SW2G_KRYLOV_GMRES (default; needs SW2G_PC_AMG or SW2G_PC_BILU0) or SW2G_KRYLOV_BICGSTAB */
+    double tol_nonlin_rel;    /* > 0: Newton residual test relative to the step's initial residual max-norm,
+                                 max|R| <= tol_nonlin_rel * max|R0| (replaces tol_nonlin); 0 (default): the
+                                 reference's absolute test */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's
@@ -82,6 +86,8 @@ typedef struct {
     double resid_l2;          /* final sqrt(sum R^2)/ndofs */
     double inc_max;           /* last max |increment| */
     double initial_resid_max; /* max |R| at the initial guess */
+    double prev_resid_max;    /* max |R| at the previous-step state (the reference's initial guess) */
+    int guess_used;           /* 1: the sw2g_set_guess guess had the smaller residual and started Newton */
 } sw2g_newton_stats;
 
 /* --- lifetime ------------------------------------------------------------ */
@@ -160,7 +166,8 @@ int sw2g_reset_profile(sw2g_model *m);
 /* Times `reps` launches of one kernel on the resident data (CUDA events on the
  * model's stream) and returns the mean launch time and the algorithmic bytes of
  * one launch: 0 FP64 SpMV, 1 FD Jacobian element kernels, 2 element residual,
- * 3 Jacobian gather, 4 AMG level-0 smoothing sweep.  Instrumentation for roofline
+ * 3 Jacobian gather, 4 AMG level-0 smoothing sweep (FP64), 5 the same sweep on FP32
+ * values and vectors.  Instrumentation for roofline
  * reporting; no counterpart in the reference. */
 int sw2g_time_kernel(sw2g_model *m, int which, int reps, double *avg_ms, double *bytes);
 
