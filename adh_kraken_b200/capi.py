@@ -24,6 +24,7 @@ EXPORTED = [
     "sw2g_assemble_jacobian", "sw2g_prepare_system", "sw2g_solve_linear_sys_bcgstab", "sw2g_fe_newton",
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
+    "sw2g_assemble_residual_noalloc",
 ]
 
 

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <mutex>
 #include <vector>
 #include <algorithm>
 #include <string>
@@ -1301,5 +1302,64 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
         case 4: *bytes = 12.0 * nnz + 20.0 * n + 24.0 * n + 16.0 * n; break;    // SpMV + block-Jacobi apply
         case 5: *bytes = 8.0 * nnz + 12.0 * n + 12.0 * n + 8.0 * n; break;      // FP32-value SpMV + FP32 block apply
     }
+    return SW2G_OK;
+}
+
+// ------------------------------------------------------------------ residual without allocation
+// For callers that cannot allocate device memory when they call in: an application
+// that hands all free device memory to its own pool at start-up, or a time loop
+// that must not allocate (or free) inside its steps.  sw2g_assemble_residual keeps
+// its element-residual and wet/dry work buffers in memory that sw2g_create
+// allocated; this variant keeps them in file-scope device arrays of a fixed size
+// instead, so a call allocates nothing.  Every GPU that loads the library holds
+// these arrays (about 10.5 MB) until the process exits.
+constexpr int kNoAllocMaxElems = 1 << 17;   // triangles + boundary segments
+constexpr int kNoAllocMaxNodes = 1 << 17;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_na_elem_resid[9 * (size_t)kNoAllocMaxElems];
+static __device__ __align__(256) int g_na_wd_flags[kNoAllocMaxElems];
+static __device__ __align__(256) int g_na_node_work[kNoAllocMaxNodes];
+// device addresses of the arrays, looked up once per device (host code may not use
+// the arrays' names as addresses: those are host-side stand-ins)
+struct NoAllocScratch { double* er; int* wd; int* node; };
+static NoAllocScratch g_na_ptr[kNoAllocMaxDevices];
+static bool g_na_ready[kNoAllocMaxDevices];
+static std::mutex g_na_mutex;
+
+static int noalloc_scratch(NoAllocScratch* out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) { g_err = "sw2g_assemble_residual_noalloc: device index too large"; return SW2G_ERR_ARG; }
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_ready[dev]) {
+        NoAllocScratch p{};
+        CK(cudaGetSymbolAddress((void**)&p.er, g_na_elem_resid));
+        CK(cudaGetSymbolAddress((void**)&p.wd, g_na_wd_flags));
+        CK(cudaGetSymbolAddress((void**)&p.node, g_na_node_work));
+        g_na_ptr[dev] = p;
+        g_na_ready[dev] = true;
+    }
+    *out = g_na_ptr[dev];
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_assemble_residual_noalloc(sw2g_model* m, const double* d_sol, const double* d_sol_old,
+                                              const double* d_sol_older, double* d_residual) {
+    NEED(m && d_sol && d_sol_old && d_sol_older && d_residual, "sw2g_assemble_residual_noalloc: null argument");
+    if (m->Etot > kNoAllocMaxElems || m->V > kNoAllocMaxNodes) {
+        g_err = "sw2g_assemble_residual_noalloc: the mesh has more than 131072 elements or nodes (the size of its "
+                "fixed work arrays); use sw2g_assemble_residual";
+        return SW2G_ERR_ARG;
+    }
+    NoAllocScratch S{};
+    TRY(noalloc_scratch(&S));
+    // every entry of the three arrays that the gather reads is written first by this call
+    // (wet/dry node marks, element flags, 9 (6) residual entries per triangle (segment)), so
+    // nothing needs clearing between calls
+    launch_wd_flags(m->M, d_sol, d_sol_old, S.node, S.wd, m->st);
+    launch_elem_resid(m->M, m->P, d_sol, d_sol_old, d_sol_older, S.wd, S.er, m->st);
+    launch_gather_resid(m->V, m->A, S.er, d_residual, m->st);
+    CKL();
+    CK(cudaStreamSynchronize(m->st));
     return SW2G_OK;
 }

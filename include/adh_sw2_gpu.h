@@ -141,6 +141,22 @@ int sw2g_solve_linear_sys_bcgstab(sw2g_model *m, double *x, const double *vals, 
 int sw2g_fe_newton(sw2g_model *m, double *sol, const double *sol_old, const double *sol_older, int *bc_mask,
                    const double *dirichlet, const sw2g_newton_opts *opts, sw2g_newton_stats *stats);
 
+/* The residual of sw2g_assemble_residual, on device buffers, for callers that cannot
+ * allocate device memory when they call in (an application that gave all free device
+ * memory to its own pool at start-up, a time loop that must not allocate inside its
+ * steps).  No counterpart in the reference.  The call allocates nothing: its work
+ * arrays are fixed-size device arrays inside the library (about 10.5 MB, held by every
+ * GPU that loads it until the process exits), so the mesh may have at most 131072
+ * elements (triangles + segments) and 131072 nodes; larger meshes get SW2G_ERR_ARG.
+ * d_sol, d_sol_old, d_sol_older [ndofs] and d_residual [ndofs] are device pointers on
+ * the model's device; the step parameters come from sw2g_set_step.  The first call on a
+ * device looks the arrays' device addresses up (once per device); make it before any
+ * stream capture.  Every call shares the arrays, so calls that overlap on the GPU
+ * (other models, streams or host threads) race; the call returns after its kernels
+ * have finished on the model's stream. */
+int sw2g_assemble_residual_noalloc(sw2g_model *m, const double *d_sol, const double *d_sol_old,
+                                   const double *d_sol_older, double *d_residual);
+
 /* --- device-resident time stepping --------------------------------------- */
 int sw2g_load_state(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
                     const int *bc_mask, const double *dirichlet);
