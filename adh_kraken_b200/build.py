@@ -26,6 +26,7 @@ UNITS = [
     ("ilu_kernels.cu", []),
     ("amg_kernels.cu", []),
     ("gmres_kernels.cu", []),
+    ("gnn_kernels.cu", []),
     ("sw2_capi.cu", []),
 ]
 

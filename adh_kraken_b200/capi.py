@@ -25,6 +25,9 @@ EXPORTED = [
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
     "sw2g_assemble_residual_noalloc",
+    # include/adh_sw2_gnn.h (learned initial guess)
+    "sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
+    "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj",
 ]
 
 
@@ -51,7 +54,8 @@ class NewtonStats(C.Structure):
     _fields_ = [("newton_its", C.c_int), ("krylov_its", C.c_int), ("linesearch_cuts", C.c_int),
                 ("refine_passes", C.c_int), ("success", C.c_int), ("krylov_breakdowns", C.c_int),
                 ("resid_max", C.c_double), ("resid_l2", C.c_double), ("inc_max", C.c_double),
-                ("initial_resid_max", C.c_double), ("prev_resid_max", C.c_double), ("guess_used", C.c_int)]
+                ("initial_resid_max", C.c_double), ("prev_resid_max", C.c_double), ("guess_used", C.c_int),
+                ("initial_resid_l2", C.c_double), ("guess_fallback", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -979,8 +979,9 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
     if (!std::isfinite(rl2)) { g_err = "non-finite residual at the initial guess"; return SW2G_ERR_NONFINITE; }
     st.prev_resid_max = rmax;
     // Initial-guess hook (after initialize_system): a supplied guess replaces the
-    // previous-step state only if its residual max-norm is smaller -- the Newton
-    // residual judges the guess, the previous step is the fallback.
+    // previous-step state only if its residual L2 norm is smaller -- the Newton
+    // residual judges the guess, the previous step is the fallback.  (L2, not the
+    // max-norm: one node's spike must not veto a guess that is better everywhere else.)
     if (o_in.use_guess && m->guess_set) {
         CK(cudaMemcpyAsync(m->d_sol, m->d_guess, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
         {
@@ -991,7 +992,11 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
         double gmax, gl2, gi;
         TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
         TRY(do_norms(m, m->d_res, m->d_dsol, &gmax, &gl2, &gi));
-        if (std::isfinite(gl2) && gmax < rmax) {
+        static const bool trace = getenv("SW2G_TRACE_NEWTON") != nullptr;
+        if (trace)
+            fprintf(stderr, "guess judge: l2 %.6e (previous step %.6e), max %.6e (previous step %.6e)\n", gl2, rl2, gmax,
+                    rmax);
+        if (std::isfinite(gl2) && gl2 < rl2) {
             rmax = gmax; rl2 = gl2; imax = gi; st.guess_used = 1;
         } else {   // fall back to the previous-step state
             CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
@@ -1005,6 +1010,7 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
         }
     }
     st.initial_resid_max = rmax;
+    st.initial_resid_l2 = rl2;
     sw2g_newton_opts o = o_in;   // the step's effective options
     // relative test: against the previous-step state's residual, the same reference with or without a guess
     if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = o_in.tol_nonlin_rel * st.prev_resid_max;
@@ -1221,12 +1227,33 @@ extern "C" int sw2g_set_guess(sw2g_model* m, const double* guess, int on_device)
     return SW2G_OK;
 }
 
+// Newton from a supplied guess that fails (no convergence, or a non-finite residual) is
+// repeated from the previous-step state, the reference's start; the work of both
+// attempts is counted.
+static int newton_with_fallback(sw2g_model* m, const sw2g_newton_opts& o, sw2g_newton_stats* S) {
+    sw2g_newton_stats a{};
+    int rc = newton_device(m, o, &a);
+    const bool guessed = o.use_guess && m->guess_set && a.guess_used;
+    if (guessed && (rc == SW2G_ERR_NONFINITE || (rc == SW2G_OK && !a.success))) {
+        sw2g_newton_opts o2 = o;
+        o2.use_guess = 0;
+        sw2g_newton_stats b{};
+        rc = newton_device(m, o2, &b);
+        b.newton_its += a.newton_its; b.krylov_its += a.krylov_its; b.linesearch_cuts += a.linesearch_cuts;
+        b.refine_passes += a.refine_passes; b.krylov_breakdowns += a.krylov_breakdowns;
+        b.guess_fallback = 1;
+        a = b;
+    }
+    if (S) *S = a;
+    return rc;
+}
+
 extern "C" int sw2g_fe_newton(sw2g_model* m, double* sol, const double* sol_old, const double* sol_older, int* bc_mask,
                               const double* dirichlet, const sw2g_newton_opts* opts, sw2g_newton_stats* stats) {
     NEED(m && sol && sol_old && sol_older && bc_mask, "sw2g_fe_newton: null argument");
     sw2g_newton_opts o; if (opts) o = *opts; else sw2g_default_opts(&o);
     TRY(sw2g_load_state(m, sol_old, sol_old, sol_older, bc_mask, dirichlet));
-    int rc = newton_device(m, o, stats);
+    int rc = newton_with_fallback(m, o, stats);
     CK(cudaMemcpyAsync(sol, m->d_sol, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaMemcpyAsync(bc_mask, m->d_bc_mask, sizeof(int) * m->n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));
@@ -1238,7 +1265,7 @@ extern "C" int sw2g_step(sw2g_model* m, const sw2g_newton_opts* opts, sw2g_newto
     sw2g_newton_opts o; if (opts) o = *opts; else sw2g_default_opts(&o);
     // smodel_super_prep_sol: sol_older <- sol_old <- sol (a pointer rotation)
     double* t = m->d_sol_older; m->d_sol_older = m->d_sol_old; m->d_sol_old = m->d_sol; m->d_sol = t;
-    int rc = newton_device(m, o, stats);
+    int rc = newton_with_fallback(m, o, stats);
     m->guess_set = false;
     return rc;
 }

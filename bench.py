@@ -50,7 +50,8 @@ def parse():
     p.add_argument("--ny", type=int, default=707)
     p.add_argument("--krylov-tol", type=float, default=1e-6,
                    help="inexact-Newton forcing: linear residual <= tol * Newton residual (floor tol_nonlin / 2)")
-    p.add_argument("--guess", choices=["none", "learned"], default="none")
+    p.add_argument("--guess", choices=["none", "learned"], default="learned")
+    p.add_argument("--weights", default=None, help="trained initial-guess weights (default: the committed ones)")
     p.add_argument("--tol-rel", type=float, default=1e-8,
                    help="Newton test max|R| <= tol_rel * max|R(previous step)|; 0: the reference's absolute 1e-8")
     p.add_argument("--no-plain", action="store_true")
@@ -121,6 +122,16 @@ def dist_setup(args):
     return world, rank, local, dist
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The slowest rank's value (every rank calls this at the same point)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_reference_sample(nsteps_total, skip):
     """Reference fe_newton (compiled from its C sources) on the SAMPLE_NX x SAMPLE_NY beach:
     seconds per step of steps skip..nsteps_total-1, and the sample's triangle count."""
@@ -176,7 +187,7 @@ def run_ours(args, world, rank, local, dist):
     guesser = None
     if args.guess == "learned":
         from adh_kraken_b200 import learned
-        guesser = learned.load_guesser(case)
+        guesser = learned.load_guesser(case, args.weights) if args.weights else learned.load_guesser(case)
     if guesser is not None:
         opts_fast.use_guess = 1
 
@@ -226,9 +237,7 @@ def run_ours(args, world, rank, local, dist):
         prof_ms, prof_n = sim.model.profile()
         sim.model.set_profiling(False)
         if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist)
             dist.barrier()
         return ms, hist, prof_ms, prof_n
 
@@ -297,10 +306,7 @@ def run_ours(args, world, rank, local, dist):
             e2e_fail += int(rc != 0 or not st.success)
             older_h.numpy()[:] = old_h.numpy(); old_h.numpy()[:] = sol_h.numpy()
         wall = time.perf_counter() - w0
-        if dist is not None:
-            t = torch.tensor([wall], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = max_over_ranks(wall, dist)
         e2e = {"value": world * K / wall, "unit": UNIT,
                "h2d_bytes_per_step": 3 * 8 * n + 4 * n + 8 * n + (8 * n if guesser is not None else 0),
                "d2h_bytes_per_step": 8 * n + 4 * n, "failed_steps": e2e_fail,
@@ -320,6 +326,7 @@ def run_ours(args, world, rank, local, dist):
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
     if rank != 0:
+        _cleanup(fast, plain, guesser)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -342,8 +349,11 @@ def run_ours(args, world, rank, local, dist):
         "fast_detail": {"newton_its": [h["newton_its"] for h in hist_fast],
                         "krylov_its": [h["krylov_its"] for h in hist_fast], "failed_steps": kfail,
                         "initial_resid": [h["initial_resid_max"] for h in hist_fast],
+                        "initial_resid_l2": [h.get("initial_resid_l2") for h in hist_fast],
+                        "prev_resid": [h.get("prev_resid_max") for h in hist_fast],
                         "final_resid": [h["resid_max"] for h in hist_fast],
                         "guess_used": [h.get("guess_used", 0) for h in hist_fast],
+                        "guess_fallback": [h.get("guess_fallback", 0) for h in hist_fast],
                         "class_ms": dict(zip(names, [round(float(x), 2) for x in prof_ms]))},
         "gpu_launches": int(np.sum(prof_n)),
         "clocks": clocks,
@@ -360,8 +370,22 @@ def run_ours(args, world, rank, local, dist):
     if out["plain_fp64"] is not None:
         out["speedup_vs_plain_fp64"] = ms_plain / ms_fast
     print(json.dumps(out), flush=True)
+    _cleanup(fast, plain, guesser)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _cleanup(*objs):
+    """Release device objects in a fixed order before interpreter shutdown."""
+    import torch
+    torch.cuda.synchronize()
+    for o in objs:
+        if o is None:
+            continue
+        model = getattr(o, "model", None)
+        if model is not None:
+            model.close()
+    torch.cuda.synchronize()
 
 
 def main():

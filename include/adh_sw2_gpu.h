@@ -55,7 +55,7 @@ typedef struct {
     double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
     int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
     int use_guess;            /* 1: start Newton from the buffer given to sw2g_set_guess when its residual
-                                 max-norm is below that of sol_old (else sol_old, the reference's start) */
+                                 L2 norm is below that of sol_old (else sol_old, the reference's start) */
     int precond;              /* SW2G_PC_AMG (default), SW2G_PC_BILU0 or SW2G_PC_BLOCK_JACOBI */
     int krylov_method;        /* SW2G_KRYLOV_GMRES (default; needs SW2G_PC_AMG or SW2G_PC_BILU0) or SW2G_KRYLOV_BICGSTAB */
     double tol_nonlin_rel;    /* > 0: Newton residual test relative to the step's initial residual max-norm,
@@ -87,7 +87,10 @@ typedef struct {
     double inc_max;           /* last max |increment| */
     double initial_resid_max; /* max |R| at the initial guess */
     double prev_resid_max;    /* max |R| at the previous-step state (the reference's initial guess) */
-    int guess_used;           /* 1: the sw2g_set_guess guess had the smaller residual and started Newton */
+    int guess_used;           /* 1: the sw2g_set_guess guess had the smaller residual L2 norm and started Newton */
+    double initial_resid_l2;  /* sqrt(sum R^2)/ndofs at the initial guess */
+    int guess_fallback;       /* 1: Newton from the guess failed and was repeated from the previous step
+                                 (the counts above include both attempts) */
 } sw2g_newton_stats;
 
 /* --- lifetime ------------------------------------------------------------ */

@@ -15,7 +15,7 @@ def declared_symbols():
         if fn.endswith(".h"):
             src = open(os.path.join(ROOT, "include", fn)).read()
             src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-            names |= set(re.findall(r"\b(sw2g_[a-z0-9_]+)\s*\(", src))
+            names |= set(re.findall(r"\b(sw2[gn]_[a-z0-9_]+)\s*\(", src))
     return names
 
 
