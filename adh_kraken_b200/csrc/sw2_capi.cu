@@ -945,6 +945,35 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
 // ------------------------------------------------------------------ Newton step
 // fe_newton (src/newton/fe_newton.c:44-915), serial non-PETSc branch, on the
 // resident state d_sol / d_sol_old / d_sol_older / d_bc_mask / d_dirichlet.
+// diagnostic (SW2G_TRACE_NEWTON): the first elements whose residual is not finite, with their nodal states
+static void debug_nonfinite(sw2g_model* m) {
+    std::vector<double> er(9 * (size_t)m->Etot), sol(m->n), old(m->n);
+    std::vector<int> tri(3 * (size_t)m->T), wd(m->T);
+    cudaMemcpyAsync(er.data(), m->d_ER, sizeof(double) * er.size(), cudaMemcpyDeviceToHost, m->st);
+    cudaMemcpyAsync(sol.data(), m->d_sol, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st);
+    cudaMemcpyAsync(old.data(), m->d_sol_old, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st);
+    cudaMemcpyAsync(tri.data(), m->d_tri, sizeof(int) * tri.size(), cudaMemcpyDeviceToHost, m->st);
+    cudaMemcpyAsync(wd.data(), m->d_wd, sizeof(int) * wd.size(), cudaMemcpyDeviceToHost, m->st);
+    cudaStreamSynchronize(m->st);
+    int shown = 0;
+    for (int e = 0; e < m->Etot && shown < 5; e++) {
+        bool bad = false;
+        for (int k = 0; k < 9; k++) bad |= !std::isfinite(er[9 * (size_t)e + k]);
+        if (!bad) continue;
+        shown++;
+        if (e < m->T) {
+            fprintf(stderr, "non-finite residual: triangle %d wd_flag %d\n", e, wd[e]);
+            for (int a = 0; a < 3; a++) {
+                const int nd = tri[3 * (size_t)e + a];
+                fprintf(stderr, "  node %d h %.6e u %.6e v %.6e | old h %.6e u %.6e v %.6e\n", nd, sol[3 * nd],
+                        sol[3 * nd + 1], sol[3 * nd + 2], old[3 * nd], old[3 * nd + 1], old[3 * nd + 2]);
+            }
+        } else {
+            fprintf(stderr, "non-finite residual: segment %d\n", e - m->T);
+        }
+    }
+}
+
 static bool valid_precond(int p) {
     return p == SW2G_PC_BLOCK_JACOBI || p == SW2G_PC_BILU0 || p == SW2G_PC_AMG;
 }
@@ -1040,8 +1069,8 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
         TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
         TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
         int cuts = 0;   // line search, fe_newton.c:681-741
-        // a step into a state whose residual is not finite (e.g. a depth driven below zero under the
-        // square root of the SUPG scale) is cut like a step that raised the residual
+        // a step into a state whose residual is not finite is cut like a step that raised the residual
+        // (the reference would stop with a NaN residual, newton_tools.c:344-349)
         while (rmax > o.tol_nonlin && (rl2 > old_l2 || !std::isfinite(rl2)) && cuts < o.max_linesearch_cuts) {
             {
                 ProfScope ps(m, 5, 2);
@@ -1053,7 +1082,11 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
             TRY(do_norms(m, m->d_res, m->d_dsol, &rmax, &rl2, &imax));
             cuts++;
         }
-        if (std::isnan(rl2) || std::isinf(rl2)) ok = false;
+        if (std::isnan(rl2) || std::isinf(rl2)) {
+            ok = false;
+            static const bool trace_nf = getenv("SW2G_TRACE_NEWTON") != nullptr;
+            if (trace_nf) debug_nonfinite(m);
+        }
         // a failed linear solve that left a zero increment must not read as an increment below inc_nonlin
         lin_stalled = (lin_status != 0 && !(imax > 0.0));
         st.linesearch_cuts += cuts;

@@ -440,7 +440,9 @@ __device__ __forceinline__ void body_resid(const TriData& T, double dt, double a
     if (fabs(h_wd) >= SW2_SMALL) {
         const double g_factor = (1 + 0.0) * grav;
         double hden = dmax_(h_wd, SW2_NOT_QUITE_SMALL);
-        double le = sqrt(djac * factor_old);
+        // a wet fraction that rounds below zero (an almost empty wet part) would make this NaN, as in
+        // the reference; clamped at zero, which changes nothing where the reference is finite
+        double le = sqrt(djac * (factor_old > 0.0 ? factor_old : 0.0));
         double cel2 = g_factor * hden;
         if (hden <= 0.0) cel2 = 0.;
         double sr = sqrt(vel_wd.x * vel_wd.x + vel_wd.y * vel_wd.y + cel2 + SW2_SMALL);

@@ -43,7 +43,7 @@ SAMPLE_NX, SAMPLE_NY = 240, 60            # reference CPU sample: same beach, co
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--nx", type=int, default=2828)

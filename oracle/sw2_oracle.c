@@ -493,8 +493,12 @@ void sw2o_body_resid(const sw2o_model *m, const double *sol, const double *sol_o
     if (fabs(h_wd) >= SMALL) {
         double g_factor = (1 + 0.0) * grav;
         double hden = dmax(h_wd, NOT_QUITE_SMALL);
-        /* fe_get_supg_tau_sw (src/tools/get_supg_tau.c:43), le = sqrt(area) (:126) */
-        double le = sqrt(djac * factor_old);
+        /* fe_get_supg_tau_sw (src/tools/get_supg_tau.c:43), le = sqrt(area) (:126).  The wet
+         * fraction can round to a tiny negative value for an element whose wet part is almost
+         * empty (depths ~1e-13); the reference then takes the square root of a negative number
+         * and its residual turns NaN.  Clamping at zero changes nothing where the reference's
+         * result is finite. */
+        double le = sqrt(djac * (factor_old > 0.0 ? factor_old : 0.0));
         double cel2 = g_factor * hden;
         if (hden <= 0.0) cel2 = 0.;
         double sr = sqrt(vel_wd.x * vel_wd.x + vel_wd.y * vel_wd.y + cel2 + SMALL);
