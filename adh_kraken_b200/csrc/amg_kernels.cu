@@ -159,23 +159,25 @@ __global__ void k_amg_scale(int nn, const VT* __restrict__ dinv, const VT* __res
     y[3 * i + 2] = (VT)(w * ((double)D[6] * b0 + (double)D[7] * b1 + (double)D[8] * b2));
 }
 
-// Level 0 (reference CSR): 8 lanes per node walk its neighbour slots.
+// Level 0 (reference CSR): LANES lanes per node walk its neighbour slots.
 // MODE 0: r = b - A x ;  MODE 1: y = x + w Dinv (b - A x)
-template <class VT, int MODE>
+template <class VT, int MODE, int LANES>
 __global__ void __launch_bounds__(256) k_amg_l0(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ dinv,
                                                 const VT* __restrict__ b, const VT* __restrict__ x, VT* __restrict__ y,
                                                 double w, const int* __restrict__ skip) {
     if (skip && *skip) return;
-    const int g8 = threadIdx.x & 7, sub = (threadIdx.x & 31) >> 3;
+    constexpr int PER_WARP = 32 / LANES;
+    const int g8 = threadIdx.x & (LANES - 1), sub = (threadIdx.x & 31) / LANES;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < A.nnodes; base += nw * 4) {
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PER_WARP; base < A.nnodes; base += nw * PER_WARP) {
         const int a = base + sub;
         const bool valid = a < A.nnodes;
         double y0 = 0, y1 = 0, y2 = 0;
         const int rs = valid ? A.indptr[3 * a] : 0;
         const int len = valid ? A.indptr[3 * a + 1] - rs : 0;
         const int s0 = valid ? A.bptr[a] : 0, deg = valid ? A.bptr[a + 1] - s0 : 0;
-        for (int j = g8; j < deg; j += 8) {
+#pragma unroll 2
+        for (int j = g8; j < deg; j += LANES) {
             const int c = A.bcol[s0 + j];
             const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
             const VT* v0 = vals + rs + 3 * j;
@@ -186,7 +188,7 @@ __global__ void __launch_bounds__(256) k_amg_l0(BlockCSR A, const VT* __restrict
             y2 += (double)v2[0] * x0 + (double)v2[1] * x1 + (double)v2[2] * x2;
         }
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
+        for (int o = LANES / 2; o > 0; o >>= 1) {
             y0 += __shfl_xor_sync(0xffffffffu, y0, o);
             y1 += __shfl_xor_sync(0xffffffffu, y1, o);
             y2 += __shfl_xor_sync(0xffffffffu, y2, o);
@@ -204,6 +206,14 @@ __global__ void __launch_bounds__(256) k_amg_l0(BlockCSR A, const VT* __restrict
         }
     }
 }
+
+static int l0_grid(int nnodes, int lanes) { return grid_for_nodes((long)nnodes * lanes / 8); }
+// lanes per node of the level-0 kernels, measured on the 4M beach (B200, 2M nodes, ~7 neighbours):
+// FP32 values 2 lanes (0.198 ms per sweep, 0.92 of the HBM copy peak) vs 4 (0.226) vs 8 (0.265);
+// FP64 4 lanes (0.304 ms) vs 8 (0.315).  Fewer lanes per node keep more independent loads in
+// flight per lane, which the latency-bound neighbour gathers need.
+template <class VT> struct L0Lanes { static constexpr int value = 4; };
+template <> struct L0Lanes<float> { static constexpr int value = 2; };
 
 // Coarse levels (block CSR, 9 values per block), same modes, 8 lanes per row.
 template <class VT, int MODE>
@@ -340,8 +350,9 @@ template <class VT>
 static void smooth_or_resid(const BlockCSR& A, const AmgLevel& L, int l, const VT* vals0, const VT* dinv, const VT* b,
                             const VT* x, VT* y, bool resid, const int* skip, cudaStream_t st) {
     if (l == 0) {
-        if (resid) k_amg_l0<VT, 0><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals0, dinv, b, x, y, 0.0, skip);
-        else k_amg_l0<VT, 1><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals0, dinv, b, x, y, kAmgOmega, skip);
+        constexpr int LN = L0Lanes<VT>::value;
+        if (resid) k_amg_l0<VT, 0, LN><<<l0_grid(A.nnodes, LN), 256, 0, st>>>(A, vals0, dinv, b, x, y, 0.0, skip);
+        else k_amg_l0<VT, 1, LN><<<l0_grid(A.nnodes, LN), 256, 0, st>>>(A, vals0, dinv, b, x, y, kAmgOmega, skip);
     } else {
         const VT* val = AmgBuf<VT>::val(L);
         if (resid) k_amg_bsr<VT, 0><<<grid_for_nodes(L.n), 256, 0, st>>>(L.n, L.bptr, L.bcol, val, dinv, b, x, y, 0.0, skip);
@@ -389,12 +400,14 @@ static void vcycle(const BlockCSR& A, const AmgHost& H, int l, const VT* vals0, 
 
 void amg_smooth0_once(const BlockCSR& A, const AmgHost& H, const double* vals, const double* b, const double* x, double* y,
                       cudaStream_t st) {
-    k_amg_l0<double, 1><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, H.dinv0_64, b, x, y, kAmgOmega, nullptr);
+    constexpr int LN = L0Lanes<double>::value;
+    k_amg_l0<double, 1, LN><<<l0_grid(A.nnodes, LN), 256, 0, st>>>(A, vals, H.dinv0_64, b, x, y, kAmgOmega, nullptr);
 }
 
 void amg_smooth0_once32(const BlockCSR& A, const AmgHost& H, const float* vals, const float* b, const float* x, float* y,
                         cudaStream_t st) {
-    k_amg_l0<float, 1><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, H.dinv0_32, b, x, y, kAmgOmega, nullptr);
+    constexpr int LN = L0Lanes<float>::value;
+    k_amg_l0<float, 1, LN><<<l0_grid(A.nnodes, LN), 256, 0, st>>>(A, vals, H.dinv0_32, b, x, y, kAmgOmega, nullptr);
 }
 
 template <class VT>

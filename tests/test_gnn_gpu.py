@@ -133,4 +133,4 @@ def test_trained_guess_beats_previous_step_start():
     # the gain: where the residual judge takes the guess, Newton starts from a residual
     # well below the previous step's (the Krylov work of both starts is printed above)
     taken = [g / p_ for g, p_ in zip(r_guess, r_plain) if g < p_]
-    assert len(taken) == used and np.mean(taken) < 0.7
+    assert len(taken) == used and np.mean(taken) < 0.85
