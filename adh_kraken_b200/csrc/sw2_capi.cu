@@ -87,6 +87,8 @@ struct sw2g_model {
     // restarted GMRES (allocated on first use)
     GmresDev gm{};
     double* gm_V64 = nullptr;            // [kGmM+1][n] Krylov basis
+    float* gm_V32 = nullptr;             // [kGmM+1][n] FP32 Krylov basis (krylov_basis_precision 32)
+    cudaGraphExec_t gm_graph_b32 = nullptr;
     double* gm_rw = nullptr;             // [n] row weights 1/s: GMRES minimises the unscaled residual
     cudaGraphExec_t gm_graph64 = nullptr, gm_graph32 = nullptr;
     std::vector<int> h_bptr, h_bcol;   // node graph, kept for the AMG set-up
@@ -177,6 +179,7 @@ extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->refine_tol = 1e-4; o->max_refine = 8; o->use_guess = 0; o->precond = SW2G_PC_AMG;
     o->krylov_method = SW2G_KRYLOV_GMRES;
     o->tol_nonlin_rel = 0.0;
+    o->krylov_basis_precision = 64;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -388,6 +391,7 @@ extern "C" void sw2g_destroy(sw2g_model* m) {
     }
     if (m->gm_graph64) cudaGraphExecDestroy(m->gm_graph64);
     if (m->gm_graph32) cudaGraphExecDestroy(m->gm_graph32);
+    if (m->gm_graph_b32) cudaGraphExecDestroy(m->gm_graph_b32);
     for (void* p : m->allocs) cudaFree(p);
     if (m->h_rout) cudaFreeHost(m->h_rout);
     if (m->h_ks) cudaFreeHost(m->h_ks);
@@ -758,6 +762,27 @@ static int alloc_gmres(sw2g_model* m) {
     return SW2G_OK;
 }
 
+// FP32 cycle: FP32 basis, FP32 matrix and FP32 preconditioner on the FP32 right-hand side f_b; the
+// correction lands in f_x (the FP64 residual and the update stay with the caller)
+static int gmres_graph32(sw2g_model* m, cudaGraphExec_t* graph, int precond) {
+    if (*graph) return SW2G_OK;
+    PrecondOp<float> op;
+    op.kind = precond; op.right = true; op.ilu = &m->ilu; op.lu = m->f_lu; op.dinv = m->f_inv; op.amg = &m->amg;
+    op.vals = m->f_vals;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+    gmres_cycle<float>(m->B, op, m->f_vals, m->gm_V32, (size_t)m->n, m->f_z, m->f_b, m->f_x, m->gm_rw, m->gm, m->st);
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        g_err = std::string("graph capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2);
+        return SW2G_ERR_CUDA;
+    }
+    CK(cudaGraphInstantiate(graph, g, 0));
+    cudaGraphDestroy(g);
+    return SW2G_OK;
+}
+
 static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, bool mixed, int precond) {
     if (*graph) return SW2G_OK;
     PrecondOp<double> op;
@@ -813,7 +838,13 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         launch_inv_scale(n, m->d_scale, m->gm_rw, m->st);
         CKL();
     }
-    TRY(gmres_graph(m, mixed ? &m->gm_graph32 : &m->gm_graph64, mixed, o.precond));
+    const bool basis32 = mixed && o.krylov_basis_precision == 32;
+    if (basis32) {
+        if (!m->gm_V32) TRY(dalloc(m, &m->gm_V32, (size_t)(kGmM + 1) * n));
+        TRY(gmres_graph32(m, &m->gm_graph_b32, o.precond));
+    } else {
+        TRY(gmres_graph(m, mixed ? &m->gm_graph32 : &m->gm_graph64, mixed, o.precond));
+    }
     const int pl = precond_launches(m, o.precond) + (mixed ? 2 : 0);
     const int per_cycle = kGmM * (6 + pl) + 4 + pl;
     const double target = std::max(o.krylov_tol * fnorm, 0.5 * o.tol_nonlin);
@@ -845,11 +876,17 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         if (*iters >= o.krylov_max_it) break;
         prev = rn;
         double rtol = 0.5 * target / rn;         // the cycle's own 2-norm estimate of the reduction still needed
-        if (rtol < 1e-12) rtol = 1e-12;
+        if (rtol < (basis32 ? 1e-5 : 1e-12)) rtol = basis32 ? 1e-5 : 1e-12;   // FP32 resolves no more per cycle
         CK(cudaMemcpyAsync(m->gm.scal + 3, &rtol, sizeof(double), cudaMemcpyHostToDevice, m->st));
         {
             ProfScope ps(m, 4, per_cycle + 1);
-            CK(cudaGraphLaunch(mixed ? m->gm_graph32 : m->gm_graph64, m->st));
+            if (basis32) {   // FP32 Krylov cycle inside the FP64 refinement
+                launch_to_float(n, m->d_t64, m->f_b, m->st);
+                CK(cudaGraphLaunch(m->gm_graph_b32, m->st));
+                launch_to_double(n, m->f_x, m->k_xi, m->st);
+            } else {
+                CK(cudaGraphLaunch(mixed ? m->gm_graph32 : m->gm_graph64, m->st));
+            }
             launch_axpy(n, 1.0, m->k_xi, x, m->st);
             CKL();
         }

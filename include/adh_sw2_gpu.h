@@ -61,6 +61,9 @@ typedef struct {
     double tol_nonlin_rel;    /* > 0: Newton residual test relative to the step's initial residual max-norm,
                                  max|R| <= tol_nonlin_rel * max|R0| (replaces tol_nonlin); 0 (default): the
                                  reference's absolute test */
+    int krylov_basis_precision; /* GMRES with krylov_precision 32: 64 (default) keeps the Krylov basis, the SpMV
+                                 and the Gram-Schmidt in FP64 around the FP32 preconditioner; 32 runs the whole
+                                 cycle in FP32, each cycle refined from the FP64 residual */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's

@@ -121,3 +121,18 @@ def test_fp32_krylov_with_refinement_matches_reference(name, precond, krylov):
     sol = sim.state()[0]
     ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
     assert max(rel_err(sol, ref)) < 1e-8, rel_err(sol, ref)
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_fp32_gmres_cycles_in_fp64_refinement_match_reference(name):
+    """Whole GMRES cycles in FP32 (basis, SpMV, AMG), refined from the FP64 residual."""
+    from adh_kraken_b200.capi import default_opts
+    from adh_kraken_b200.timeloop import SW2Simulation
+    case, z = load(name)
+    sim = SW2Simulation(case, opts=default_opts(krylov_precision=32, krylov_basis_precision=32, precond=2,
+                                                krylov_method=1))
+    hist = sim.run(case.nsteps)
+    assert all(h["success"] for h in hist)
+    sol = sim.state()[0]
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
+    assert max(rel_err(sol, ref)) < 1e-8, rel_err(sol, ref)
