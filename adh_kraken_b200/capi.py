@@ -41,7 +41,7 @@ class NewtonOpts(C.Structure):
                 ("max_linesearch_cuts", C.c_int), ("krylov_max_it", C.c_int), ("krylov_tol", C.c_double),
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
                 ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int),
-                ("tol_nonlin_rel", C.c_double), ("krylov_basis_precision", C.c_int)]
+                ("tol_nonlin_rel", C.c_double), ("krylov_basis_precision", C.c_int), ("krylov_restart", C.c_int)]
 
 PC_BLOCK_JACOBI = 0
 PC_BILU0 = 1

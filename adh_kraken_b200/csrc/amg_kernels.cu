@@ -222,14 +222,16 @@ __global__ void __launch_bounds__(256) k_amg_bsr(int n, const int* __restrict__ 
                                                  const VT* __restrict__ b, const VT* __restrict__ x, VT* __restrict__ y,
                                                  double w, const int* __restrict__ skip) {
     if (skip && *skip) return;
-    const int g8 = threadIdx.x & 7, sub = (threadIdx.x & 31) >> 3;
+    constexpr int LANES = sizeof(VT) == 4 ? 4 : 8, PER_WARP = 32 / LANES;   // coarse rows hold ~10 blocks
+    const int g8 = threadIdx.x & (LANES - 1), sub = (threadIdx.x & 31) / LANES;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < n; base += nw * 4) {
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PER_WARP; base < n; base += nw * PER_WARP) {
         const int a = base + sub;
         const bool valid = a < n;
         double y0 = 0, y1 = 0, y2 = 0;
         const int q0 = valid ? bptr[a] : 0, q1 = valid ? bptr[a + 1] : 0;
-        for (int q = q0 + g8; q < q1; q += 8) {
+#pragma unroll 2
+        for (int q = q0 + g8; q < q1; q += LANES) {
             const int c = bcol[q];
             const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
             const VT* v = val + 9 * (size_t)q;
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(256) k_amg_bsr(int n, const int* __restrict__ 
             y2 += (double)v[6] * x0 + (double)v[7] * x1 + (double)v[8] * x2;
         }
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
+        for (int o = LANES / 2; o > 0; o >>= 1) {
             y0 += __shfl_xor_sync(0xffffffffu, y0, o);
             y1 += __shfl_xor_sync(0xffffffffu, y1, o);
             y2 += __shfl_xor_sync(0xffffffffu, y2, o);

@@ -228,12 +228,13 @@ __global__ void k_gm_combine(int n, const VT* __restrict__ Vb, size_t ld, VT* __
 
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st) {
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m) {
     const int n = A.n, g = gm_grid(n);
     const int* done = G.state;
     k_gm_start<VT><<<g, 256, 0, st>>>(n, rhs, rw, G);
     k_gm_v0<VT><<<g, 256, 0, st>>>(n, rhs, rw, Vb, G);
-    for (int j = 0; j < kGmM; j++) {
+    if (m < 1 || m > kGmM) m = kGmM;
+    for (int j = 0; j < m; j++) {
         VT* vj = Vb + (size_t)j * ld;
         VT* w = Vb + (size_t)(j + 1) * ld;
         copy_skip<VT>(n, vj, z, done, st);
@@ -249,8 +250,8 @@ void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* 
     precond_apply<VT>(A, P, out, nullptr, st);
 }
 template void gmres_cycle<double>(const BlockCSR&, const PrecondOp<double>&, const double*, double*, size_t, double*,
-                                  const double*, double*, const double*, const GmresDev&, cudaStream_t);
+                                  const double*, double*, const double*, const GmresDev&, cudaStream_t, int);
 template void gmres_cycle<float>(const BlockCSR&, const PrecondOp<float>&, const float*, float*, size_t, float*,
-                                 const float*, float*, const double*, const GmresDev&, cudaStream_t);
+                                 const float*, float*, const double*, const GmresDev&, cudaStream_t, int);
 
 }  // namespace sw2

@@ -540,16 +540,20 @@ template <class VT>
 __global__ void __launch_bounds__(256) k_spmv(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ x,
                                               VT* __restrict__ y, const int* __restrict__ skip) {
     if (skip && *skip) return;
-    const int g8 = threadIdx.x & 7, sub = (threadIdx.x & 31) >> 3;
+    // lanes per node: 8 for FP64 values; 2 for FP32, whose half-size rows need more neighbour
+    // blocks in flight per lane (the same choice as the AMG level-0 kernels, measured there)
+    constexpr int LANES = sizeof(VT) == 4 ? 2 : 8, PER_WARP = 32 / LANES;
+    const int g8 = threadIdx.x & (LANES - 1), sub = (threadIdx.x & 31) / LANES;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < A.nnodes; base += nw * 4) {
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PER_WARP; base < A.nnodes; base += nw * PER_WARP) {
         const int a = base + sub;
         const bool valid = a < A.nnodes;
         double y0 = 0, y1 = 0, y2 = 0;
         const int rs = valid ? A.indptr[3 * a] : 0;
         const int len = valid ? A.indptr[3 * a + 1] - rs : 0;
         const int s0 = valid ? A.bptr[a] : 0, deg = valid ? A.bptr[a + 1] - s0 : 0;
-        for (int j = g8; j < deg; j += 8) {
+#pragma unroll 2
+        for (int j = g8; j < deg; j += LANES) {
             const int b = A.bcol[s0 + j];
             const double xb0 = x[3 * b], xb1 = x[3 * b + 1], xb2 = x[3 * b + 2];
             const VT* v0 = vals + rs + 3 * j;
@@ -560,7 +564,7 @@ __global__ void __launch_bounds__(256) k_spmv(BlockCSR A, const VT* __restrict__
             y2 += (double)v2[0] * xb0 + (double)v2[1] * xb1 + (double)v2[2] * xb2;
         }
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
+        for (int o = LANES / 2; o > 0; o >>= 1) {
             y0 += __shfl_xor_sync(0xffffffffu, y0, o);
             y1 += __shfl_xor_sync(0xffffffffu, y1, o);
             y2 += __shfl_xor_sync(0xffffffffu, y2, o);

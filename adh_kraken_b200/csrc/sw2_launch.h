@@ -167,7 +167,8 @@ template <class VT>
 void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st);
 
 // ---- restarted GMRES(m) cycle (gmres_kernels.cu)
-constexpr int kGmM = 30;                // Krylov dimension of one cycle
+constexpr int kGmM = 50;                // largest Krylov dimension of one cycle (buffers, register arrays)
+constexpr int kGmDefault = 30;          // default restart length
 struct GmresDev {                       // device buffers of one cycle
     double* H = nullptr;                // [kGmM][kGmM+1] Hessenberg columns (rotated in place)
     double* cs = nullptr; double* sn = nullptr;   // [kGmM] Givens rotations
@@ -182,7 +183,7 @@ struct GmresDev {                       // device buffers of one cycle
 // residual 2-norm; Vb holds kGmM+1 vectors of stride ld
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st);
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m);
 // rw_i = 1 / s_i (weights that make a scaled system's residual the unscaled one)
 void launch_inv_scale(int n, const double* scale, double* rw, cudaStream_t st);
 template <class VT>

@@ -56,6 +56,7 @@ def parse():
                    help="Newton test max|R| <= tol_rel * max|R(previous step)|; 0: the reference's absolute 1e-8")
     p.add_argument("--basis", type=int, choices=[32, 64], default=32,
                    help="fast path: FP32 (default) or FP64 GMRES basis around the FP32 preconditioner")
+    p.add_argument("--restart", type=int, default=50, help="GMRES restart length of both paths (1..50)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -183,7 +184,8 @@ def run_ours(args, world, rank, local, dist):
     K, W = args.steps, args.warmup
     case = beach_case(nx=args.nx, ny=args.ny, nsteps=W + 2 * K + 4)
     base = dict(tol_nonlin=1e-8, tol_nonlin_rel=args.tol_rel, inc_nonlin=1e-6, max_nonlin_it=10,
-                krylov_max_it=20000, krylov_tol=args.krylov_tol, precond=2, krylov_method=1)
+                krylov_max_it=20000, krylov_tol=args.krylov_tol, precond=2, krylov_method=1,
+                krylov_restart=args.restart)
     opts_fast = default_opts(krylov_precision=32, krylov_basis_precision=args.basis, **base)
     opts_plain = default_opts(krylov_precision=64, **base)
     guesser = None
@@ -340,7 +342,7 @@ def run_ours(args, world, rank, local, dist):
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": "beach4M", "ntri": case.ntri, "nnodes": case.nnodes, "ndofs": 3 * case.nnodes,
                    "nnz": fast.model.nnz, "dt_s": case.dt, "tol_nonlin": 1e-8, "tol_nonlin_rel": args.tol_rel,
-                   "krylov": "GMRES(30)+AMG",
+                   "krylov": f"GMRES({args.restart})+AMG",
                    "krylov_forcing": args.krylov_tol, "guess": args.guess if guesser is not None else "none",
                    "fast_precision": ("AMG preconditioner FP32, Krylov/residual/FD FP64" if args.basis == 64 else
                                       "GMRES cycle (basis, SpMV, AMG) FP32 inside FP64 refinement; residual/FD FP64"),

@@ -64,6 +64,7 @@ typedef struct {
     int krylov_basis_precision; /* GMRES with krylov_precision 32: 64 (default) keeps the Krylov basis, the SpMV
                                  and the Gram-Schmidt in FP64 around the FP32 preconditioner; 32 runs the whole
                                  cycle in FP32, each cycle refined from the FP64 residual */
+    int krylov_restart;       /* GMRES restart length, 1..50 (default 30) */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's
