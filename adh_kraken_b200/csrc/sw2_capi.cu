@@ -1376,13 +1376,13 @@ extern "C" int sw2g_reset_profile(sw2g_model* m) {
 }
 
 extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_ms, double* bytes) {
-    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 5, "sw2g_time_kernel: bad argument");
+    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 6, "sw2g_time_kernel: bad argument");
     const double nnz = m->nnz, n = m->n, T = m->T, S = m->S;
     if (which >= 4) {   // the AMG sweeps
         if (!m->amg_ready) TRY(build_amg(m));
         amg_setup(m->B, m->amg, m->A, m->d_vals, m->st);
     }
-    if (which == 5) {
+    if (which == 5 || which == 6) {
         TRY(alloc_fp32(m));
         launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
     }
@@ -1394,6 +1394,7 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
             case 3: launch_gather_jac(m->A, m->d_EJ, m->Etot, m->d_vals, m->st); break;
             case 4: amg_smooth0_once(m->B, m->amg, m->d_vals, m->k_p, m->k_Ap, m->k_As, m->st); break;
             case 5: amg_smooth0_once32(m->B, m->amg, m->f_vals, m->f_p, m->f_Ap, m->f_As, m->st); break;
+            case 6: amg_apply<float>(m->B, m->amg, m->f_vals, m->f_Ap, nullptr, m->st); break;
 
         }
     };
@@ -1415,6 +1416,7 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
         case 2: *bytes = 316.0 * T + 200.0 * S + 8.0 * n; break;            // element inputs + residual out
         case 3: *bytes = 8.0 * 81.0 * T + 8.0 * 36.0 * S + 12.0 * nnz; break;   // element blocks in, CSR values + map out
         case 4: *bytes = 12.0 * nnz + 20.0 * n + 24.0 * n + 16.0 * n; break;    // SpMV + block-Jacobi apply
+        case 6: *bytes = 4.0 * (8.0 * nnz + 32.0 * n); break;   // ~4 level-0 matrix passes (coarse levels extra)
         case 5: *bytes = 8.0 * nnz + 12.0 * n + 12.0 * n + 8.0 * n; break;   // FP32 SpMV + FP32 block apply
     }
     return SW2G_OK;

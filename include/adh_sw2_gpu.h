@@ -190,7 +190,8 @@ int sw2g_reset_profile(sw2g_model *m);
  * model's stream) and returns the mean launch time and the algorithmic bytes of
  * one launch: 0 FP64 SpMV, 1 FD Jacobian element kernels, 2 element residual,
  * 3 Jacobian gather, 4 AMG level-0 smoothing sweep (FP64), 5 the same sweep on FP32
- * values and vectors.  Instrumentation for roofline
+ * values and vectors, 6 one FP32 AMG V-cycle (bytes: its four level-0 matrix passes).
+ * Instrumentation for roofline
  * reporting; no counterpart in the reference. */
 int sw2g_time_kernel(sw2g_model *m, int which, int reps, double *avg_ms, double *bytes);
 
