@@ -24,7 +24,7 @@ EXPORTED = [
     "sw2g_assemble_jacobian", "sw2g_prepare_system", "sw2g_solve_linear_sys_bcgstab", "sw2g_fe_newton",
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
-    "sw2g_assemble_residual_noalloc",
+    "sw2g_assemble_residual_noalloc", "sw2g_grid_mass",
     # include/adh_sw2_gnn.h (learned initial guess)
     "sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
     "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj",
@@ -235,6 +235,19 @@ class SW2Model:
         a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
         self._check(lib().sw2g_device_state(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def grid_mass(self, sol=None, density=1.0, dt=None, elem=False):
+        """(density * grid mass, one step's boundary mass inflow[, per-triangle terms]) of
+        `sol` (host [ndofs]) or, with sol None, of the resident state."""
+        out = np.zeros(2)
+        em = np.zeros(max(self.case.ntri, 1)) if elem else None
+        dt = self.case.dt if dt is None else dt
+        src = None if sol is None else _f64(sol)
+        self._check(lib().sw2g_grid_mass(self.h, _d(src) if src is not None else None, C.c_double(density),
+                                         C.c_double(dt), _d(out), _d(em) if em is not None else None))
+        if elem:
+            return out[0], out[1], em[: self.case.ntri]
+        return out[0], out[1]
 
     def set_profiling(self, on=True):
         self._check(lib().sw2g_set_profiling(self.h, int(on)))

@@ -1357,6 +1357,29 @@ extern "C" int sw2g_step(sw2g_model* m, const sw2g_newton_opts* opts, sw2g_newto
     return rc;
 }
 
+extern "C" int sw2g_grid_mass(sw2g_model* m, const double* sol, double density, double dt, double* out,
+                              double* elem_mass) {
+    NEED(m && out, "sw2g_grid_mass: null argument");
+    NEED(dt >= 0.0, "sw2g_grid_mass: negative dt");
+    const double* d = m->d_sol;
+    if (sol) {   // a host state goes to a work vector: the resident state stays as it is
+        CK(cudaMemcpyAsync(m->d_t64, sol, sizeof(double) * m->n, cudaMemcpyHostToDevice, m->st));
+        d = m->d_t64;
+    }
+    {
+        ProfScope ps(m, 5, 1);
+        Reduce R{m->d_partial, m->d_counter, m->d_rout};
+        launch_mass_balance(m->M, d, density, density * dt, elem_mass ? m->d_ER : nullptr, R, m->st);
+        CKL();
+    }
+    CK(cudaMemcpyAsync(m->h_rout, m->d_rout, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->st));
+    if (elem_mass && m->T)
+        CK(cudaMemcpyAsync(elem_mass, m->d_ER, sizeof(double) * m->T, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    out[0] = m->h_rout[0]; out[1] = m->h_rout[1];
+    return SW2G_OK;
+}
+
 extern "C" int sw2g_set_profiling(sw2g_model* m, int on) {
     NEED(m, "null model");
     m->prof = on != 0;

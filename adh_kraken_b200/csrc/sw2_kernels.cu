@@ -205,6 +205,126 @@ __global__ void k_gather_jac(AssemblyMaps A, const double* __restrict__ EJ, int 
     out[0] = a0; out[1] = a1; out[2] = a2;
 }
 
+// ---------------------------------------------------------------- mass balance
+// tl_find_grid_mass_elem2d (src/tools/tl_grid_mass.c:198-275) per triangle, with
+// the dry-vertex rule of fe_3m2d_dry_wet_factornew (:442-515): a vertex is dry when
+// its depth is strictly negative; one dry vertex adds the wet part plus the dry
+// corner's negative depth counted as positive mass, two dry vertices integrate the
+// clipped depths times the wet fraction.
+__device__ __forceinline__ double tri_mass_term(const MeshView& M, const double* __restrict__ sol, int e) {
+    const int T_ = M.ntri;
+    V2 x[3];
+    double h[3], hneg[3] = {0.0, 0.0, 0.0};
+    int passcode = 0, total = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        x[a].x = M.ex[a * T_ + e]; x[a].y = M.ey[a * T_ + e];
+        h[a] = sol[3 * M.tri[3 * e + a]];
+        const int d = (h[a] < 0.0) ? 1 : 0;
+        total += d; passcode += (d << a);
+    }
+    const double djac = M.djac[e];
+    double factor = 1.0;
+    int num_dry = total;
+    if (total == 3) factor = 0.0;
+    else if (total != 0) {
+        if (total != 1) passcode = 7 - passcode;
+        const int o = passcode / 2;
+        const double ho = sel3(h, o);
+        const V2 xo = sel3(x, o);
+        V2 nx[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (i != o) {
+                const double xsi = h[i] / (h[i] - ho);
+                nx[i].x = x[i].x + xsi * (xo.x - x[i].x);   // FIXED_POS, macro.h:756
+                nx[i].y = x[i].y + xsi * (xo.y - x[i].y);
+            } else {
+                nx[i] = x[i];
+            }
+        }
+        const double ax = nx[1].x - nx[0].x, ay = nx[1].y - nx[0].y;   // TRI_AREA, macro.h:771
+        const double bx = nx[2].x - nx[0].x, by = nx[2].y - nx[0].y;
+        const double area = (ax * by - ay * bx) / 2.0;
+        if (area / djac < SW2_SMALL) {               // a sliver of dry (one vertex) or wet (two) area
+            num_dry = (total % 2 == 1) ? 0 : 3;
+            factor = (double)(total % 2);
+        } else {
+            factor = (total >> 1) - (total % 2);
+            factor *= area / djac;
+            factor = factor + ((factor < 0) ? 1.0 : 0.0);
+        }
+    }
+    double f1 = factor, f2 = 0.0;
+    if (num_dry == 1) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) if (h[a] < 0.0) hneg[a] = h[a];
+        f1 = 1.0; f2 = -1.0 * (1.0 - factor);
+    } else if (num_dry == 2) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) if (h[a] < 0.0) { hneg[a] = h[a]; h[a] = 0.0; }
+    }
+    // integrate_triangle_f, src/fe/fe_integrals_2d.c:25
+    return (f1 * djac * (h[0] + h[1] + h[2]) / 3.0) + (f2 * djac * (hneg[0] + hneg[1] + hneg[2]) / 3.0);
+}
+
+// One boundary segment's mass inflow over a step (tl_grid_mass.c:310-320 with
+// integrate_line_h_f, src/fe/fe_integrals_1d.c:42): -c len/6 ((2 vn0 + vn1) h0 + (vn0 + 2 vn1) h1),
+// c = density dt, vn = v . n at the two nodes.
+__device__ __forceinline__ double seg_mass_flux(const MeshView& M, const double* __restrict__ sol, int k, double c) {
+    double vn[2], h[2];
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+        const int nd = M.seg[2 * k + a];
+        vn[a] = sol[3 * nd + 1] * M.snx[k] + sol[3 * nd + 2] * M.sny[k];
+        h[a] = sol[3 * nd];
+    }
+    const double t1 = M.sdjac[k] * SW2_ONE_6 * c;
+    return -(t1 * ((2 * vn[0] + vn[1]) * h[0] + (vn[0] + 2 * vn[1]) * h[1]));
+}
+
+// Grid-stride over triangles then segments; per-block sums in a fixed order and a
+// last-block pass over the block partials in block order (run-to-run deterministic).
+// out[0] = density * mass, out[1] = boundary inflow; elem_mass (optional) = per-triangle terms.
+__global__ void __launch_bounds__(256) k_mass_balance(MeshView M, const double* __restrict__ sol, double density,
+                                                      double c, double* __restrict__ elem_mass,
+                                                      double* __restrict__ partial, unsigned int* __restrict__ counter,
+                                                      double* __restrict__ out) {
+    __shared__ double sh[2][8];
+    __shared__ bool is_last;
+    double mass = 0.0, flux = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M.ntri; e += stride) {
+        const double t = tri_mass_term(M, sol, e);
+        if (elem_mass) elem_mass[e] = t;
+        mass += t;
+    }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M.nseg; k += stride) flux += seg_mass_flux(M, sol, k, c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mass += __shfl_xor_sync(0xffffffffu, mass, o);
+        flux += __shfl_xor_sync(0xffffffffu, flux, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[0][w] = mass; sh[1][w] = flux; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < 8; i++) { a += sh[0][i]; b += sh[1][i]; }
+        partial[4 * blockIdx.x] = a; partial[4 * blockIdx.x + 1] = b;
+        __threadfence();
+        const unsigned int t = atomicInc(counter, gridDim.x - 1);   // the last block wraps it back to 0
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)gridDim.x; k++) { a += __ldcg(partial + 4 * k); b += __ldcg(partial + 4 * k + 1); }
+        out[0] = a * density;
+        out[1] = b;
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static inline int blocks(long n, int b) { return (int)((n + b - 1) / b); }
 
@@ -247,6 +367,15 @@ void launch_elem_jac(const MeshView& M, const StepParams& P, const double* sol, 
 
 void launch_gather_jac(const AssemblyMaps& A, const double* EJ, int Etot, double* vals, cudaStream_t st) {
     if (A.nblocks) k_gather_jac<<<blocks(3L * A.nblocks, 256), 256, 0, st>>>(A, EJ, Etot, vals);
+}
+
+void launch_mass_balance(const MeshView& M, const double* sol, double density, double density_dt, double* elem_mass,
+                         Reduce R, cudaStream_t st) {
+    long work = M.ntri > M.nseg ? M.ntri : M.nseg;
+    int g = blocks(work, 256);
+    if (g > kMaxBlocks) g = kMaxBlocks;
+    if (g < 1) g = 1;
+    k_mass_balance<<<g, 256, 0, st>>>(M, sol, density, density_dt, elem_mass, R.partial, R.counter, R.out);
 }
 
 }  // namespace sw2

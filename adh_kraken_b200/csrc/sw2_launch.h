@@ -36,6 +36,12 @@ struct Reduce {           // reduction workspace (device)
 };
 constexpr int kMaxBlocks = 1184;   // 8 x 148 SMs
 
+// Mass balance of a state: out[0] = density * grid mass (tl_find_grid_mass_elem2d,
+// src/tools/tl_grid_mass.c:198), out[1] = the step's boundary mass inflow with
+// density_dt = density * dt (tl_grid_mass.c:310-320); elem_mass (optional) [ntri].
+void launch_mass_balance(const MeshView& M, const double* sol, double density, double density_dt, double* elem_mass,
+                         Reduce R, cudaStream_t st);
+
 // Newton norms over non-Dirichlet dofs: out[0] = max|res|, out[1] = sum res^2,
 // out[2] = max|dsol| (get_residual_norms, src/newton/newton_tools.c:303-373)
 void launch_norms(int n, const double* res, const double* dsol, const int* bc_mask, Reduce R, cudaStream_t st);

@@ -70,6 +70,7 @@ class SW2Simulation:
         sol0 = case.sol0.astype(np.float64)
         self.model.load_state(sol0, sol0, sol0)
         self.history = []
+        self.mass_log = None
 
     def bc_values(self, t1, t2):
         s = self.case.series
@@ -91,7 +92,30 @@ class SW2Simulation:
         st = self.model.step(opts or self.opts)
         self.t = t_new
         self.history.append(st)
+        if self.mass_log is not None:
+            m, inflow = self.model.grid_mass(None, self.density, self.case.dt)
+            self.inflow_total += inflow
+            self.mass_log.append((t_new, m, inflow))
         return st
+
+    def start_mass_balance(self, density=1.0):
+        """Start the mass bookkeeping of tl_find_grid_mass_error_elem2d
+        (src/tools/tl_grid_mass.c:280) from the resident state: every later step
+        records the grid mass of its result and its boundary mass inflow."""
+        self.density = float(density)
+        self.mass0, _ = self.model.grid_mass(None, self.density, self.case.dt)
+        self.inflow_total = 0.0
+        self.mass_log = []
+
+    def mass_balance(self):
+        """Grid mass now, at the start, the boundary inflow since, and the reference's
+        mass error |mass - inflow - initial mass|."""
+        if self.mass_log is None:
+            raise RuntimeError("start_mass_balance() was not called")
+        m = self.mass_log[-1][1] if self.mass_log else self.mass0
+        err = abs(m - self.inflow_total - self.mass0)
+        return {"initial_mass": self.mass0, "mass": m, "inflow": self.inflow_total, "error": err,
+                "rel_error": err / self.mass0 if self.mass0 else None, "steps": len(self.mass_log)}
 
     def run(self, nsteps, opts=None, stop_on_failure=True):
         for _ in range(nsteps):

@@ -226,6 +226,7 @@ def run_ours(args, world, rank, local, dist):
     def timed(sim, stepper, clocks=None):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         hist = []
+        sim.start_mass_balance(1000.0)          # water density, kg/m^3
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
@@ -350,7 +351,8 @@ def run_ours(args, world, rank, local, dist):
         "plain_fp64": None if ms_plain is None else {
             "value": world * K / (ms_plain * 1e-3), "ms_per_step": ms_plain / K,
             "newton_its": [h["newton_its"] for h in hist_plain], "krylov_its": [h["krylov_its"] for h in hist_plain],
-            "failed_steps": sum(1 for h in hist_plain if not h["success"])},
+            "failed_steps": sum(1 for h in hist_plain if not h["success"]),
+            "mass_balance": plain.mass_balance()},
         "fast_detail": {"newton_its": [h["newton_its"] for h in hist_fast],
                         "krylov_its": [h["krylov_its"] for h in hist_fast], "failed_steps": kfail,
                         "initial_resid": [h["initial_resid_max"] for h in hist_fast],
@@ -359,7 +361,8 @@ def run_ours(args, world, rank, local, dist):
                         "final_resid": [h["resid_max"] for h in hist_fast],
                         "guess_used": [h.get("guess_used", 0) for h in hist_fast],
                         "guess_fallback": [h.get("guess_fallback", 0) for h in hist_fast],
-                        "class_ms": dict(zip(names, [round(float(x), 2) for x in prof_ms]))},
+                        "class_ms": dict(zip(names, [round(float(x), 2) for x in prof_ms])),
+                        "mass_balance": fast.mass_balance()},
         "gpu_launches": int(np.sum(prof_n)),
         "clocks": clocks,
         "roofline": {"kernel": "k_amg_l0<float,1> (AMG level-0 smoothing sweep, FP32)", "bound": "hbm",

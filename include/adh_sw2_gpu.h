@@ -148,6 +148,20 @@ int sw2g_solve_linear_sys_bcgstab(sw2g_model *m, double *x, const double *vals, 
 int sw2g_fe_newton(sw2g_model *m, double *sol, const double *sol_old, const double *sol_older, int *bc_mask,
                    const double *dirichlet, const sw2g_newton_opts *opts, sw2g_newton_stats *stats);
 
+/* Mass balance of a state.  out[0] = tl_find_grid_mass_elem2d(density, .., depth, grid, ..)
+ * (src/tools/tl_grid_mass.c:198): density times the sum over triangles of the depth
+ * integral, with the reference's dry-vertex rule (depth < 0 is dry).  out[1] = one
+ * step's boundary mass inflow, the boundary loop of tl_find_grid_mass_error_elem2d
+ * (tl_grid_mass.c:310-320): -density dt sum over boundary segments of the integral of
+ * h (v . n), each segment with its own length (the reference takes the first
+ * segment's length for all of them).  The reference's mass error after k steps is
+ * |out[0] - (sum of the k inflows) - initial mass|.  sol: host [ndofs], or NULL for
+ * the resident state (after sw2g_step / sw2g_load_state); elem_mass: optional host
+ * [ntri], each triangle's term before the density factor.  The sums run in a fixed
+ * order (run-to-run identical); they differ from the reference's serial sum only by
+ * rounding. */
+int sw2g_grid_mass(sw2g_model *m, const double *sol, double density, double dt, double *out, double *elem_mass);
+
 /* The residual of sw2g_assemble_residual, on device buffers, for callers that cannot
  * allocate device memory when they call in (an application that gave all free device
  * memory to its own pool at start-up, a time loop that must not allocate inside its

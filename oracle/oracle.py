@@ -171,6 +171,22 @@ class OracleModel:
         return lib().sw2o_bicgstab_bj(self.ndof, _i(self.indptr), _i(self.cols), _d(vals), _d(x), _d(b),
                                       _d(scale_vect), max_it, C.c_double(tol))
 
+    def grid_mass(self, sol, density=1.0):
+        f = lib().sw2o_grid_mass
+        f.restype = C.c_double
+        return f(C.byref(self.m), _d(sol), C.c_double(density))
+
+    def elem_mass(self, sol):
+        f = lib().sw2o_elem_mass
+        f.restype = C.c_double
+        return np.array([f(C.byref(self.m), _d(sol), e) for e in range(self.case.ntri)])
+
+    def boundary_mass_flux(self, sol, density=1.0, dt=None, first_seg_length=False):
+        f = lib().sw2o_boundary_mass_flux
+        f.restype = C.c_double
+        dt = self.case.dt if dt is None else dt
+        return f(C.byref(self.m), _d(sol), C.c_double(density), C.c_double(dt), int(first_seg_length))
+
     def newton(self, sol, sol_old, sol_older, bc_mask, dirichlet, krylov_max_it=100, krylov_tol=1e-11):
         c = self.case
         stats = np.zeros(4)

@@ -36,7 +36,7 @@
  *  (vi)  selem1d_init_alloc_array writes through node arrays it never allocated
  *        (selem_1d.c:86-125); see build_grid.
  *
- * Usage: adh_ref_harness <dump|run|time> <case.bin> <out.bin> [every|reps]
+ * Usage: adh_ref_harness <dump|run|time|mass> <case.bin> <out.bin> [every|reps]
  *        adh_ref_harness rect - <out.bin> xmin xmax ymin ymax npx npy a0 ax
  */
 #include "adh.h"
@@ -369,6 +369,29 @@ static void mode_time(const CASE *c, int reps) {
     out_rec("assembly_seconds", 'd', v, 3);
 }
 
+/* The reference's mass-balance tools on the case state (density 1, no flags):
+ * tl_find_grid_mass_elem2d (src/tools/tl_grid_mass.c:198) of sol and of sol_old,
+ * and tl_find_grid_mass_error_elem2d (tl_grid_mass.c:280) of sol with sol_old's
+ * mass as the initial mass, which also returns one step's boundary mass flux. */
+static void mode_mass(const CASE *c) {
+    SMODEL_SUPER *sm = g_sm; SGRID *grid = sm->grid; int V = grid->nnodes;
+    int *ih = sm->ivars[sm->ivar_pos.var[adh_def._H]];
+    int *iu = sm->ivars[sm->ivar_pos.var[adh_def._UDA]], *iv = sm->ivars[sm->ivar_pos.var[adh_def._VDA]];
+    double *head = malloc(sizeof(double) * V), *head_old = malloc(sizeof(double) * V);
+    SVECT2D *vel = malloc(sizeof(SVECT2D) * V);
+    for (int i = 0; i < V; i++) {
+        head[i] = sm->sol[ih[i]]; head_old[i] = sm->sol_old[ih[i]];
+        vel[i].x = sm->sol[iu[i]]; vel[i].y = sm->sol[iv[i]];
+    }
+    SFLAGS flags; memset(&flags, 0, sizeof flags);
+    double m_new = tl_find_grid_mass_elem2d(1.0, NULL, NULL, head, grid, flags);
+    double m_old = tl_find_grid_mass_elem2d(1.0, NULL, NULL, head_old, grid, flags);
+    double flux_T = 0.;
+    double err = tl_find_grid_mass_error_elem2d(1.0, head, vel, grid, flags, m_old, NULL, NULL, c->dt, &flux_T);
+    double v[4] = {m_new, m_old, flux_T, err};
+    out_rec("grid_mass", 'd', v, 4);
+}
+
 /* The reference's own structured-grid generator (src/tools/create_rectangular_grid.c:4),
  * used to pin the flume mesh builder: argv = xmin xmax ymin ymax npx npy a0 ax. */
 static void mode_rect(int argc, char **argv) {
@@ -416,6 +439,7 @@ int main(int argc, char **argv) {
     if (strcmp(argv[1], "dump") == 0) mode_dump(&c);
     else if (strcmp(argv[1], "run") == 0) mode_run(&c, argc > 4 ? atoi(argv[4]) : 1);
     else if (strcmp(argv[1], "time") == 0) mode_time(&c, argc > 4 ? atoi(argv[4]) : 1);
+    else if (strcmp(argv[1], "mass") == 0) mode_mass(&c);
     else { fprintf(stderr, "harness: unknown mode %s\n", argv[1]); return 2; }
     fclose(g_out);
     return 0;

@@ -889,3 +889,101 @@ int sw2o_newton(sw2o_model *m, double *sol, const double *sol_old, const double 
     free(res); free(dsol); free(vals); free(sv);
     return success;
 }
+
+/* ------------------------------------------------------------------ mass balance */
+
+/* fe_3m2d_dry_wet_factornew, src/tools/tl_grid_mass.c:442-515: the wet fraction
+ * of a triangle for the mass integral.  Unlike the residual's wet/dry factor, a
+ * vertex is dry only when its depth is strictly negative (:462). */
+static double mass_wet_factor(const v2 *x, const double *h, double djac, int *num_dry) {
+    int passcode = 0, total = 0;
+    for (int i = 0; i < 3; i++) { int d = (h[i] < 0.0) ? 1 : 0; total += d; passcode += (d << i); }
+    if (total == 3) { *num_dry = 3; return 0.0; }
+    if (total == 0) { *num_dry = 0; return 1.0; }
+    if (total != 1) passcode = 7 - passcode;
+    int only = passcode / 2;
+    v2 nx[3];
+    for (int i = 0; i < 3; i++) {
+        if (i != only) {
+            double xsi = h[i] / (h[i] - h[only]);
+            nx[i].x = x[i].x + xsi * (x[only].x - x[i].x);           /* FIXED_POS, macro.h:756 */
+            nx[i].y = x[i].y + xsi * (x[only].y - x[i].y);
+        } else nx[i] = x[i];
+    }
+    double elem_djac = djac;
+    double ax = nx[1].x - nx[0].x, ay = nx[1].y - nx[0].y;           /* TRI_AREA, macro.h:771 */
+    double bx = nx[2].x - nx[0].x, by = nx[2].y - nx[0].y;
+    djac = (ax * by - ay * bx) / 2.0;
+    if (djac / elem_djac < SMALL) {                                   /* :506-509 */
+        int odd = total % 2;
+        *num_dry = (odd == 1) ? 0 : 3;
+        return (double)odd;
+    }
+    double factor = (total >> 1) - (total % 2);
+    *num_dry = total;
+    factor *= djac / elem_djac;
+    return factor + ((factor < 0) ? 1.0 : 0.0);
+}
+
+/* integrate_triangle_f, src/fe/fe_integrals_2d.c:25 */
+static inline double tri_int_f(double djac, double c, const double *f) {
+    return (c * djac * (f[0] + f[1] + f[2]) / 3.0);
+}
+
+double sw2o_elem_mass(const sw2o_model *m, const double *sol, int e) {
+    /* one triangle's term of tl_find_grid_mass_elem2d, src/tools/tl_grid_mass.c:209-258 */
+    double head[3], hneg[3] = {0.0, 0.0, 0.0};
+    v2 x[3];
+    for (int a = 0; a < 3; a++) {
+        int nd = m->tri[3 * e + a];
+        head[a] = sol[3 * nd];
+        x[a].x = m->xyz[3 * nd]; x[a].y = m->xyz[3 * nd + 1];
+    }
+    double djac = m->tri_djac[e];
+    int num_dry;
+    double factor = mass_wet_factor(x, head, djac, &num_dry);
+    double f1, f2;
+    switch (num_dry) {
+        case 1:     /* the wet part plus the (negative) dry vertex depth counted as positive mass */
+            for (int a = 0; a < 3; a++) if (head[a] < 0.0) hneg[a] = head[a];
+            f1 = 1.0; f2 = -1.0 * (1.0 - factor);
+            break;
+        case 2:
+            for (int a = 0; a < 3; a++) if (head[a] < 0.0) { hneg[a] = head[a]; head[a] = 0.0; }
+            f1 = factor; f2 = 0.0;
+            break;
+        default:
+            f1 = factor; f2 = 0.0;
+            break;
+    }
+    return tri_int_f(djac, f1, head) + tri_int_f(djac, f2, hneg);
+}
+
+double sw2o_grid_mass(const sw2o_model *m, const double *sol, double density) {
+    double mass = 0.0;
+    for (int e = 0; e < m->ntri; e++) mass += sw2o_elem_mass(m, sol, e);
+    return mass * density;
+}
+
+double sw2o_boundary_mass_flux(const sw2o_model *m, const double *sol, double density, double dt,
+                                int first_seg_length) {
+    /* the boundary loop of tl_find_grid_mass_error_elem2d, src/tools/tl_grid_mass.c:310-320:
+     * minus the integral of h (v . n) over every boundary segment, times density dt
+     * (inflow positive).  Each segment uses its own length; the reference passes the
+     * first segment's length (grid->elem1d->djac, :318) for all of them, which
+     * first_seg_length = 1 reproduces. */
+    double total = 0.0;
+    for (int k = 0; k < m->nseg; k++) {
+        double vn[2], h[2];
+        for (int a = 0; a < 2; a++) {
+            int nd = m->seg[2 * k + a];
+            vn[a] = sol[3 * nd + 1] * m->seg_nrml[2 * k] + sol[3 * nd + 2] * m->seg_nrml[2 * k + 1];
+            h[a] = sol[3 * nd];
+        }
+        /* integrate_line_h_f, src/fe/fe_integrals_1d.c:42, with h = v . n and f = depth */
+        double len = first_seg_length ? m->seg_djac[0] : m->seg_djac[k];
+        double t1 = len * one_6 * (density * dt);
+        total -= (t1 * ((2 * vn[0] + vn[1]) * h[0] + (vn[0] + 2 * vn[1]) * h[1]));
+    }
+    return total;
+}

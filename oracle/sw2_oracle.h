@@ -90,6 +90,16 @@ int sw2o_newton(sw2o_model *m, double *sol, const double *sol_old, const double 
                 int max_nonlin_it, int max_linesearch_cuts, int krylov_max_it, double krylov_tol,
                 double *stats);
 
+/* mass balance: tl_find_grid_mass_elem2d (src/tools/tl_grid_mass.c:198) of the depths in sol,
+ * one triangle's term of it, and one step's boundary mass flux (inflow positive) of the
+ * boundary loop of tl_find_grid_mass_error_elem2d (tl_grid_mass.c:310-320); that loop
+ * weights every segment by the first segment's length, which first_seg_length = 1
+ * reproduces (0: each segment's own length, what the CUDA path computes) */
+double sw2o_grid_mass(const sw2o_model *m, const double *sol, double density);
+double sw2o_elem_mass(const sw2o_model *m, const double *sol, int e);
+double sw2o_boundary_mass_flux(const sw2o_model *m, const double *sol, double density, double dt,
+                                int first_seg_length);
+
 /* flop counter for one unperturbed triangle residual evaluation (fully wet path) */
 long sw2o_body_resid_flops(void);
 

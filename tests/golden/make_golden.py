@@ -58,11 +58,47 @@ def run_fixture(name, case):
     np.savez_compressed(os.path.join(HERE, name), **arrs)
 
 
+def mass_states(case, seed, run_name=None):
+    """State triples for the mass-balance fixture: perturbed states, one with nodes
+    at exactly zero depth and at -1e-20 (the near-empty dry-corner branch of
+    fe_3m2d_dry_wet_factornew), and the reference run's last kept state."""
+    out = [perturbed_states(case, seed)]
+    sol, sol_old, sol_older = perturbed_states(case, seed + 1)
+    rng = np.random.default_rng(seed + 2)
+    nodes = rng.choice(case.nnodes, size=max(2, case.nnodes // 8), replace=False)
+    half = len(nodes) // 2
+    sol[3 * nodes[:half]] = 0.0
+    sol[3 * nodes[half:]] = -1e-20
+    out.append((sol, sol_old, sol_older))
+    if run_name is not None:
+        z = np.load(os.path.join(HERE, run_name))
+        kept = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)
+        last = kept[-1].copy()
+        prev = kept[-2].copy() if len(kept) > 1 else case.sol0.copy()
+        out.append((last, prev, prev))
+    return out
+
+
+def mass_fixture(name, case, seed, run_name=None):
+    states = mass_states(case, seed, run_name)
+    res = []
+    for sol, sol_old, sol_older in states:
+        d = run_harness("mass", case, sol=sol, sol_old=sol_old, sol_older=sol_older)
+        res.append(d["grid_mass"])
+    arrs = case_arrays(case)
+    arrs["sol"] = np.stack([s[0] for s in states])
+    arrs["sol_old"] = np.stack([s[1] for s in states])
+    arrs["ref_grid_mass"] = np.stack(res)   # per state: mass(sol), mass(sol_old), boundary flux, mass error
+    np.savez_compressed(os.path.join(HERE, name), **arrs)
+
+
 def main():
     dump_fixture("dump_flume_21x6.npz", flume_case(nsteps=1, npx=21, npy=6), seed=11)
     dump_fixture("dump_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=12)
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
+    mass_fixture("mass_flume_21x6.npz", flume_case(nsteps=8, npx=21, npy=6), 31, "run_flume_21x6_8steps.npz")
+    mass_fixture("mass_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=4), 41, "run_wetdry_12_4steps.npz")
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
