@@ -24,7 +24,7 @@ EXPORTED = [
     "sw2g_assemble_jacobian", "sw2g_prepare_system", "sw2g_solve_linear_sys_bcgstab", "sw2g_fe_newton",
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
-    "sw2g_assemble_residual_noalloc", "sw2g_grid_mass",
+    "sw2g_assemble_residual_noalloc", "sw2g_grid_mass", "sw2g_undo_step",
     # include/adh_sw2_gnn.h (learned initial guess)
     "sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
     "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj",
@@ -230,6 +230,9 @@ class SW2Model:
         st = NewtonStats()
         self._check(lib().sw2g_step(self.h, C.byref(opts or default_opts()), C.byref(st)))
         return st.as_dict()
+
+    def undo_step(self):
+        self._check(lib().sw2g_undo_step(self.h))
 
     def device_state(self):
         a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()

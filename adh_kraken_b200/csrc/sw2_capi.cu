@@ -63,6 +63,7 @@ struct sw2g_model {
     double *d_sol = nullptr, *d_sol_old = nullptr, *d_sol_older = nullptr, *d_dirichlet = nullptr, *d_guess = nullptr;
     int *d_bc_mask = nullptr, *d_mask_save = nullptr;
     bool guess_set = false;
+    bool can_undo = false;   // the levels were rotated by the last sw2g_step
     // work
     int *d_wd = nullptr, *d_node_tmp = nullptr;
     double *d_ER = nullptr, *d_EJ = nullptr, *d_res = nullptr, *d_vals = nullptr, *d_dsol = nullptr;
@@ -1164,6 +1165,7 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
 
 static int put3(sw2g_model* m, const double* sol, const double* sol_old, const double* sol_older) {
     const size_t b = sizeof(double) * m->n;
+    m->can_undo = false;
     CK(cudaMemcpyAsync(m->d_sol, sol, b, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_sol_old, sol_old, b, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(m->d_sol_older, sol_older, b, cudaMemcpyHostToDevice, m->st));
@@ -1352,9 +1354,22 @@ extern "C" int sw2g_step(sw2g_model* m, const sw2g_newton_opts* opts, sw2g_newto
     sw2g_newton_opts o; if (opts) o = *opts; else sw2g_default_opts(&o);
     // smodel_super_prep_sol: sol_older <- sol_old <- sol (a pointer rotation)
     double* t = m->d_sol_older; m->d_sol_older = m->d_sol_old; m->d_sol_old = m->d_sol; m->d_sol = t;
+    m->can_undo = true;
     int rc = newton_with_fallback(m, o, stats);
     m->guess_set = false;
     return rc;
+}
+
+extern "C" int sw2g_undo_step(sw2g_model* m) {
+    NEED(m, "sw2g_undo_step: null model");
+    NEED(m->can_undo, "sw2g_undo_step: no sw2g_step to undo since the state was loaded or last undone");
+    NEED(m->P.alpha == 0.0, "sw2g_undo_step: the three-level scheme (tau_temporal != 0) needs the sol_older level, "
+                            "which the step overwrote");
+    // the step's rotation was sol_older <- sol_old <- sol <- (sol_older's buffer); turn it back.  The
+    // start state and its previous level were never written by the step; sol_older's buffer was.
+    double* c = m->d_sol; m->d_sol = m->d_sol_old; m->d_sol_old = m->d_sol_older; m->d_sol_older = c;
+    m->can_undo = false;
+    return SW2G_OK;
 }
 
 extern "C" int sw2g_grid_mass(sw2g_model* m, const double* sol, double density, double dt, double* out,

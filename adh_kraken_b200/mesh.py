@@ -170,6 +170,23 @@ def flume_case(nsteps: int = 100, npx: int = 101, npy: int = 11) -> SW2Case:
     return SW2Case("flume", xyz, tri, seg, kind, sol0, dt, nsteps, series)
 
 
+def still_beach_case(nsteps: int = 1440, npx: int = 16, npy: int = 6, nt: int = 1440) -> SW2Case:
+    """Still water on a sloping beach, the reference's wet/dry test
+    (src/test/test_sw2_wd.c:40-166): 1000 m x 500 m rectangular grid, bed
+    z = 0.0015 x, water level 1 m (h0 = 1 - z, dry where x > 666.7 m), u = v = 0,
+    no boundary segments (a closed basin), dt = 864000 s / nt.  The water must stay
+    at rest and keep its mass."""
+    xyz, tri = rectangular_grid(0.0, 1000.0, 0.0, 500.0, npx, npy, a0=0.0, ax=0.0015)
+    V = xyz.shape[0]
+    sol0 = np.zeros(3 * V)
+    sol0[0::3] = 1.0 - xyz[:, 2]
+    dt = 864000.0 / nt
+    tf = dt * max(nsteps, 1)
+    series = {0: _const_series(0.0, tf, 0.0), 1: _const_series(0.0, tf, 0.0), 2: _const_series(0.0, tf, 0.0)}
+    return SW2Case("still_beach", xyz, tri, np.zeros((0, 2), np.int32), np.zeros(0, np.int32), sol0, dt, nsteps,
+                   series)
+
+
 def _edge_chains(ii, jj, nx, ny):
     """Node chains of the four rectangle edges (x-major numbering)."""
     idx = np.arange(nx * ny).reshape(nx, ny)

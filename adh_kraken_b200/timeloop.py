@@ -10,9 +10,11 @@ from __future__ import annotations
 
 import numpy as np
 
-from .capi import SW2Model, default_opts
+from .capi import SW2Error, SW2Model, default_opts
 
 _EPS = np.finfo(np.float64).eps
+DT_REDUCE_FACTOR = 0.25        # tc_scale's factor after a failed Newton solve (src/include/define.h:127)
+NOT_QUITE_SMALL = float(np.finfo(np.float32).eps)   # update_dt's end-of-run slack (src/include/define.h:32)
 
 
 def _interval(times, t):
@@ -61,9 +63,9 @@ def series_step_average(times, values, t1, t2):
 class SW2Simulation:
     """A time-stepping SW2 run whose state stays resident on the GPU."""
 
-    def __init__(self, case, opts=None, stream=None):
+    def __init__(self, case, opts=None, stream=None, model=None):
         self.case = case
-        self.model = SW2Model(case, stream=stream)
+        self.model = model if model is not None else SW2Model(case, stream=stream)
         self.opts = opts or default_opts(tol_nonlin=case.tol_nonlin, inc_nonlin=case.inc_nonlin,
                                          max_nonlin_it=case.max_nonlin_it)
         self.t = case.t0
@@ -79,24 +81,57 @@ class SW2Simulation:
             out.append(series_step_average(*s[k], t1, t2) if k in s else 0.0)
         return out
 
-    def prepare_step(self):
+    def prepare_step(self, dt=None):
         """update_dt + the series averaging of advance_time for the next step."""
-        dt = self.case.dt
+        dt = self.case.dt if dt is None else dt
         t_new = self.t + dt
         d, vx, vy = self.bc_values(t_new - dt, t_new)
         self.model.set_step(dt, d, vx, vy)
         return t_new
 
-    def step(self, opts=None):
-        t_new = self.prepare_step()
+    def step(self, opts=None, dt=None):
+        """One Newton solve over [t, t + dt] (dt: the case's step by default).  A failed
+        solve leaves the state at the step's start, as fe_newton does, and time moves on."""
+        dt = self.case.dt if dt is None else dt
+        t_new = self.prepare_step(dt)
         st = self.model.step(opts or self.opts)
         self.t = t_new
         self.history.append(st)
-        if self.mass_log is not None:
-            m, inflow = self.model.grid_mass(None, self.density, self.case.dt)
+        if self.mass_log is not None and st["success"]:
+            m, inflow = self.model.grid_mass(None, self.density, dt)
             self.inflow_total += inflow
             self.mass_log.append((t_new, m, inflow))
         return st
+
+    def advance(self, opts=None, max_cuts=3):
+        """One step of the case's dt that survives failed Newton solves.  A failed
+        solve is undone and the interval is tried again with dt scaled by
+        DT_REDUCE_FACTOR, as tc_scale scales it (src/tools/tc_scale.c:10, called at
+        src/newton/fe_newton.c:887); the rest of the interval is then covered in
+        steps of the reduced size.  The reference instead ends its time loop at the
+        first failure (src/timeloop/time_loop.c:37).  Gives up after max_cuts
+        reductions (success 0, the state at the last good substep)."""
+        target = self.t + self.case.dt
+        dt, cuts, subs = self.case.dt, 0, []
+        while self.t + NOT_QUITE_SMALL * self.case.dt < target:
+            h = min(dt, target - self.t)
+            t_start = self.t
+            try:
+                st = self.step(opts, dt=h)
+            except SW2Error:               # a non-finite residual: a failed solve like any other
+                st = {"success": 0}
+            if st["success"]:
+                subs.append(st)
+                continue
+            self.model.undo_step()
+            self.t = t_start
+            cuts += 1
+            if cuts > max_cuts:
+                break
+            dt = h * DT_REDUCE_FACTOR
+        ok = cuts <= max_cuts
+        return {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts,
+                "newton_its": sum(s["newton_its"] for s in subs), "krylov_its": sum(s["krylov_its"] for s in subs)}
 
     def start_mass_balance(self, density=1.0):
         """Start the mass bookkeeping of tl_find_grid_mass_error_elem2d

@@ -187,6 +187,16 @@ int sw2g_set_guess(sw2g_model *m, const double *guess, int guess_on_device);
 /* One time step on the resident state: smodel_super_prep_sol (sol_older <- sol_old
  * <- sol) then fe_newton, as advance_time does (src/timeloop/time_loop.c:56-89). */
 int sw2g_step(sw2g_model *m, const sw2g_newton_opts *opts, sw2g_newton_stats *stats);
+/* Undo the last sw2g_step: the levels go back to what they were before it (sol =
+ * the step's start state, sol_old = its previous level), so that the same interval
+ * can be tried again, e.g. with a smaller dt after a failed Newton solve.  The
+ * reference instead scales dt by DT_REDUCE_FACTOR (tc_scale, src/tools/tc_scale.c:10,
+ * called at src/newton/fe_newton.c:887) and ends its time loop (time_loop.c:37).
+ * The step overwrote the sol_older level, so this is refused (SW2G_ERR_ARG) under
+ * the three-level scheme (tau_temporal != 0), after sw2g_load_state or any entry
+ * point that loads states, and a second time in a row.  The permanent Dirichlet
+ * marks the step added stay, as they do in the reference. */
+int sw2g_undo_step(sw2g_model *m);
 /* Device pointers of the resident state (for device-side consumers such as the
  * learned initial-guess network). */
 int sw2g_device_state(sw2g_model *m, double **sol, double **sol_old, double **sol_older);

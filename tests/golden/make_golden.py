@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from adh_kraken_b200.mesh import flume_case, small_delaunay_case  # noqa: E402
+from adh_kraken_b200.mesh import flume_case, small_delaunay_case, still_beach_case  # noqa: E402
 from oracle.refio import run_harness  # noqa: E402
 
 
@@ -51,8 +51,8 @@ def dump_fixture(name, case, seed):
     np.savez_compressed(os.path.join(HERE, name), **arrs)
 
 
-def run_fixture(name, case):
-    r = run_harness("run", case)
+def run_fixture(name, case, every=1):
+    r = run_harness("run", case, extra=(every,))
     arrs = case_arrays(case)
     arrs.update({f"ref_{k}": v for k, v in r.items() if k != "step_seconds"})
     np.savez_compressed(os.path.join(HERE, name), **arrs)
@@ -97,6 +97,7 @@ def main():
     dump_fixture("dump_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=12)
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
+    run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)
     mass_fixture("mass_flume_21x6.npz", flume_case(nsteps=8, npx=21, npy=6), 31, "run_flume_21x6_8steps.npz")
     mass_fixture("mass_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=4), 41, "run_wetdry_12_4steps.npz")
     for f in sorted(os.listdir(HERE)):

@@ -136,3 +136,52 @@ def test_fp32_gmres_cycles_in_fp64_refinement_match_reference(name):
     sol = sim.state()[0]
     ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
     assert max(rel_err(sol, ref)) < 1e-8, rel_err(sol, ref)
+
+
+def test_still_beach_kat_matches_reference():
+    """Still water on a sloping beach with a dry upper part and no boundary
+    segments (src/test/test_sw2_wd.c): 1440 steps, the kept states within 1e-8 of
+    the reference's run, the water at rest, wet depths unchanged, mass kept."""
+    from adh_kraken_b200.timeloop import SW2Simulation
+    case, z = load("run_still_beach_16x6_1440steps.npz")
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)
+    sim = SW2Simulation(case)
+    kept = []
+    for k in range(case.nsteps):
+        assert sim.step()["success"]
+        if (k + 1) % 240 == 0:
+            kept.append(sim.state()[0])
+    kept = np.array(kept)
+    assert np.abs(kept - ref).max() < 1e-8
+    h0 = case.sol0[0::3]
+    wet = h0 > 0.0
+    m0 = sim.model.grid_mass(case.sol0)[0]
+    for s in kept:
+        assert np.abs(s[1::3]).sum() + np.abs(s[2::3]).sum() < 1e-7
+        assert np.abs(s[0::3][wet] - h0[wet]).sum() < 1e-7
+        assert np.abs(s[0::3][~wet]).max() < 1e-9
+        assert abs(sim.model.grid_mass(s)[0] - m0) <= 1e-12 * m0
+
+
+def test_undo_step_retries_the_interval():
+    """A failed Newton solve undone with sw2g_undo_step, then the same interval
+    again: the result is the state an unbroken first step reaches."""
+    from adh_kraken_b200.capi import SW2Error, default_opts
+    from adh_kraken_b200.timeloop import SW2Simulation
+    case, z = load("run_flume_21x6_8steps.npz")
+    a = SW2Simulation(case)
+    assert a.step()["success"]
+    sa = a.state()[0]
+    b = SW2Simulation(case)
+    st = b.step(opts=default_opts(max_nonlin_it=1, krylov_max_it=1))
+    assert not st["success"]
+    b.model.undo_step()
+    b.t -= case.dt
+    with pytest.raises(SW2Error):
+        b.model.undo_step()                  # only once per step
+    assert b.step()["success"]
+    assert max(rel_err(b.state()[0], sa)) < 1e-10
+    c = SW2Simulation(case)
+    adv = c.advance()
+    assert adv["success"] == 1 and adv["substeps"] == 1 and adv["dt_cuts"] == 0
+    assert max(rel_err(c.state()[0], sa)) < 1e-10

@@ -125,3 +125,39 @@ def test_grid_mass_covers_every_dry_branch():
         if np.any(h == -1e-20):
             seen.add("tiny")
     assert seen >= {0, 1, 2, 3, "tiny"}
+
+
+def still_beach_checks(case, states, mass_of):
+    """The still-water beach (src/test/test_sw2_wd.c:232-263): the water stays at
+    rest (sum |u| + sum |v| below the test's 1e-7), wet depths stay put, and the mass
+    is kept.  Dry nodes (h0 < 0) go to h = 0 in the first step, in the reference as
+    here, which the reference test's sum |h - h0| would count as an error."""
+    h0 = case.sol0[0::3]
+    wet = h0 > 0.0
+    m0 = mass_of(case.sol0)
+    for s in states:
+        assert np.abs(s[1::3]).sum() + np.abs(s[2::3]).sum() < 1e-7
+        assert np.abs(s[0::3][wet] - h0[wet]).sum() < 1e-7
+        assert np.abs(s[0::3][~wet]).max() < 1e-9
+        assert abs(mass_of(s) - m0) <= 1e-12 * m0
+
+
+def test_still_beach_kat_matches_reference():
+    case, z = load("run_still_beach_16x6_1440steps.npz")
+    o = OracleModel(case)
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)
+    assert z["ref_step_ok"].all() and len(ref) == 6
+    sol = case.sol0.copy(); old = sol.copy(); older = sol.copy()
+    bc_mask = np.zeros(o.ndof, np.int32); dirichlet = np.zeros(o.ndof)
+    t, kept = case.t0, []
+    for k in range(case.nsteps):
+        t += case.dt
+        older[:] = old; old[:] = sol
+        o.set_bc_window(t - case.dt, t)
+        st = o.newton(sol, old, older, bc_mask, dirichlet)
+        assert st["ok"]
+        if (k + 1) % 240 == 0:
+            kept.append(sol.copy())
+    assert np.abs(np.array(kept) - ref).max() < 1e-10
+    still_beach_checks(case, ref, o.grid_mass)
+    still_beach_checks(case, kept, o.grid_mass)
