@@ -162,7 +162,7 @@ __global__ void k_amg_scale(int nn, const VT* __restrict__ dinv, const VT* __res
 // Level 0 (reference CSR): LANES lanes per node walk its neighbour slots.
 // MODE 0: r = b - A x ;  MODE 1: y = x + w Dinv (b - A x)
 template <class VT, int MODE, int LANES>
-__global__ void __launch_bounds__(256) k_amg_l0(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ dinv,
+__global__ void __launch_bounds__(256, kSweepBlocksPerSM) k_amg_l0(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ dinv,
                                                 const VT* __restrict__ b, const VT* __restrict__ x, VT* __restrict__ y,
                                                 double w, const int* __restrict__ skip) {
     if (skip && *skip) return;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256) k_amg_l0(BlockCSR A, const VT* __restrict
     }
 }
 
-static int l0_grid(int nnodes, int lanes) { return grid_for_nodes((long)nnodes * lanes / 8); }
+static int l0_grid(int nnodes, int lanes) { return grid_resident((long)nnodes * lanes, kSweepBlocksPerSM); }
 // lanes per node of the level-0 kernels, measured on the 4M beach (B200, 2M nodes, ~7 neighbours):
 // FP32 values 2 lanes (0.198 ms per sweep, 0.92 of the HBM copy peak) vs 4 (0.226) vs 8 (0.265);
 // FP64 4 lanes (0.304 ms) vs 8 (0.315).  Fewer lanes per node keep more independent loads in
@@ -217,7 +217,7 @@ template <> struct L0Lanes<float> { static constexpr int value = 2; };
 
 // Coarse levels (block CSR, 9 values per block), same modes, 8 lanes per row.
 template <class VT, int MODE>
-__global__ void __launch_bounds__(256) k_amg_bsr(int n, const int* __restrict__ bptr, const int* __restrict__ bcol,
+__global__ void __launch_bounds__(256, kSweepBlocksPerSM) k_amg_bsr(int n, const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                  const VT* __restrict__ val, const VT* __restrict__ dinv,
                                                  const VT* __restrict__ b, const VT* __restrict__ x, VT* __restrict__ y,
                                                  double w, const int* __restrict__ skip) {
@@ -357,8 +357,9 @@ static void smooth_or_resid(const BlockCSR& A, const AmgLevel& L, int l, const V
         else k_amg_l0<VT, 1, LN><<<l0_grid(A.nnodes, LN), 256, 0, st>>>(A, vals0, dinv, b, x, y, kAmgOmega, skip);
     } else {
         const VT* val = AmgBuf<VT>::val(L);
-        if (resid) k_amg_bsr<VT, 0><<<grid_for_nodes(L.n), 256, 0, st>>>(L.n, L.bptr, L.bcol, val, dinv, b, x, y, 0.0, skip);
-        else k_amg_bsr<VT, 1><<<grid_for_nodes(L.n), 256, 0, st>>>(L.n, L.bptr, L.bcol, val, dinv, b, x, y, kAmgOmega, skip);
+        const int gb = grid_resident((long)L.n * (sizeof(VT) == 4 ? 4 : 8), kSweepBlocksPerSM);   // k_amg_bsr's lanes
+        if (resid) k_amg_bsr<VT, 0><<<gb, 256, 0, st>>>(L.n, L.bptr, L.bcol, val, dinv, b, x, y, 0.0, skip);
+        else k_amg_bsr<VT, 1><<<gb, 256, 0, st>>>(L.n, L.bptr, L.bcol, val, dinv, b, x, y, kAmgOmega, skip);
     }
 }
 

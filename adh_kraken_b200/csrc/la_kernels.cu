@@ -535,9 +535,17 @@ void launch_masked_copy(int n, const int* mask, const double* src, double* dst, 
 namespace sw2 {
 
 int grid_for_nodes(long nodes) { return grid_for(8L * nodes, 256); }
+int grid_resident(long work_items, int blocks_per_sm) {
+    grid_for(1, 256);   // fills g_num_sms
+    long need = (work_items + 255) / 256;
+    long cap = (long)blocks_per_sm * g_num_sms;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
 
 template <class VT>
-__global__ void __launch_bounds__(256) k_spmv(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ x,
+__global__ void __launch_bounds__(256, kSweepBlocksPerSM) k_spmv(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ x,
                                               VT* __restrict__ y, const int* __restrict__ skip) {
     if (skip && *skip) return;
     // lanes per node: 8 for FP64 values; 2 for FP32, whose half-size rows need more neighbour
@@ -571,6 +579,10 @@ __global__ void __launch_bounds__(256) k_spmv(BlockCSR A, const VT* __restrict__
         }
         if (g8 == 0 && valid) { y[3 * a] = (VT)y0; y[3 * a + 1] = (VT)y1; y[3 * a + 2] = (VT)y2; }
     }
+}
+// lanes per node of k_spmv (must match LANES inside it) and its one-wave grid
+template <class VT> static int spmv_grid(int nnodes) {
+    return grid_resident((long)nnodes * (sizeof(VT) == 4 ? 2 : 8), kSweepBlocksPerSM);
 }
 
 template <class VT>
@@ -650,7 +662,7 @@ __global__ void __launch_bounds__(256) k_bicg_omega(int n, KrylovVecs<VT> V, Kry
 }
 
 void launch_spmv64(const BlockCSR& A, const double* vals, const double* x, double* y, cudaStream_t st) {
-    k_spmv<double><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, x, y, nullptr);
+    k_spmv<double><<<spmv_grid<double>(A.nnodes), 256, 0, st>>>(A, vals, x, y, nullptr);
 }
 
 template <class VT>
@@ -706,11 +718,11 @@ void launch_bicg_init_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<V
         k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                // y = b
         k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.x, V.z);
         precond_apply<VT>(A, P, V.z, nullptr, st);                    // z = M^-1 y
-        k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.z, V.r, nullptr);
+        k_spmv<VT><<<spmv_grid<VT>(A.nnodes), 256, 0, st>>>(A, V.vals, V.z, V.r, nullptr);
     } else {
         precond_apply<VT>(A, P, V.b, nullptr, st);                    // b <- M^-1 b
         k_copy<VT><<<gv, 256, 0, st>>>(A.n, V.b, V.x);                // x = b
-        k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, V.vals, V.x, V.r, nullptr);
+        k_spmv<VT><<<spmv_grid<VT>(A.nnodes), 256, 0, st>>>(A, V.vals, V.x, V.r, nullptr);
         precond_apply<VT>(A, P, V.r, nullptr, st);                    // r <- M^-1 A x
     }
     k_bicg_init_pc<VT><<<gv, 256, 0, st>>>(A.n, V, S, R);
@@ -721,7 +733,7 @@ void copy_skip(int n, const VT* a, VT* b, const int* skip, cudaStream_t st) {
 }
 template <class VT>
 void spmv_skip(const BlockCSR& A, const VT* vals, const VT* x, VT* y, const int* skip, cudaStream_t st) {
-    k_spmv<VT><<<grid_for_nodes(A.nnodes), 256, 0, st>>>(A, vals, x, y, skip);
+    k_spmv<VT><<<spmv_grid<VT>(A.nnodes), 256, 0, st>>>(A, vals, x, y, skip);
 }
 template void copy_skip<double>(int, const double*, double*, const int*, cudaStream_t);
 template void copy_skip<float>(int, const float*, float*, const int*, cudaStream_t);
@@ -731,7 +743,7 @@ template void spmv_skip<float>(const BlockCSR&, const float*, const float*, floa
 template <class VT>
 void launch_bicg_iteration_pc(const BlockCSR& A, const PrecondOp<VT>& P, KrylovVecs<VT> V, KrylovScalars* S, Reduce R,
                               cudaStream_t st) {
-    const int gv = grid_for(A.n, 256), gs = grid_for_nodes(A.nnodes);
+    const int gv = grid_for(A.n, 256), gs = spmv_grid<VT>(A.nnodes);
     const int* done = &S->done;
     if (P.right) {
         k_copy_skip<VT><<<gv, 256, 0, st>>>(A.n, V.p, V.z, done);

@@ -94,6 +94,13 @@ void launch_bilu_factor(const BlockCSR& A, const IluHost& H, const double* vals,
 template <class VT>
 void launch_bilu_apply(const BlockCSR& A, const IluHost& H, const VT* lu, const VT* dinv, VT* y, cudaStream_t st);
 int grid_for_nodes(long nodes);   // grid for 8-lanes-per-node kernels
+// The node-blocked matrix kernels (level-0 and coarse AMG sweeps, SpMV) are grid-stride
+// loops of 256-thread blocks held to 40 registers by __launch_bounds__(256, kSweepBlocksPerSM):
+// 65536 / (40 x 256) = 6 blocks fit on an SM.  Their grid is exactly the blocks that are
+// resident at once, so every block runs in the first wave; a larger grid leaves a second,
+// partial wave of blocks that start only when the first ones finish.
+constexpr int kSweepBlocksPerSM = 6;
+int grid_resident(long work_items, int blocks_per_sm);   // 256-thread blocks, at most blocks_per_sm x SMs
 
 // ---- aggregation AMG over the node blocks (amg_kernels.cu)
 constexpr int kAmgMaxLevels = 10;
