@@ -43,8 +43,9 @@ __device__ __forceinline__ bool gm_last_block(const GmresDev& G) {
     __threadfence();   // every thread's partial writes are visible device-wide before the count
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned int t = atomicInc(G.counter, gridDim.x - 1);
-        is_last = (t == gridDim.x - 1);
+        const unsigned int total = gridDim.x * gridDim.y;
+        unsigned int t = atomicInc(G.counter, total - 1);
+        is_last = (t == total - 1);
     }
     __syncthreads();
     return is_last;
@@ -99,25 +100,32 @@ __global__ void k_gm_rowweight(int n, VT* __restrict__ w, const double* __restri
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = (VT)((double)w[i] * rw[i]);
 }
 
-// h_k = v_k . w for k < nv (w = v_nv before orthogonalisation), into column j of H
+// h_k = v_k . w for k < nv (w = v_nv before orthogonalisation), into column j of H.
+// blockIdx.y picks a group of kDotGroup basis vectors: each thread keeps kDotGroup
+// accumulators (about 40 registers instead of one per basis vector), so 6 blocks fit on
+// an SM and every load of the group is issued at once.  A thread's elements and the
+// reduction tree do not depend on the group, so every h_k is the same sum as with all
+// accumulators in one thread.  w is read once per group.
+constexpr int kDotGroup = 8;
 template <class VT>
 __global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __restrict__ Vb, size_t ld, int j, GmresDev G) {
     if (G.state[0]) return;
-    __shared__ double sh[8][kGmM + 1];
+    __shared__ double sh[8][kDotGroup];
+    const int k0 = blockIdx.y * kDotGroup;
     const VT* w = Vb + (size_t)nv * ld;
-    double acc[kGmM + 1];
+    double acc[kDotGroup];
 #pragma unroll
-    for (int k = 0; k <= kGmM; k++) acc[k] = 0.0;
+    for (int k = 0; k < kDotGroup; k++) acc[k] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double wi = w[i];
 #pragma unroll
-        for (int k = 0; k <= kGmM; k++)
-            if (k < nv) acc[k] += (double)Vb[(size_t)k * ld + i] * wi;
+        for (int k = 0; k < kDotGroup; k++)
+            if (k0 + k < nv) acc[k] += (double)Vb[(size_t)(k0 + k) * ld + i] * wi;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k <= kGmM; k++) {
-        if (k < nv) {
+    for (int k = 0; k < kDotGroup; k++) {
+        if (k0 + k < nv) {
             double v = acc[k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -125,10 +133,10 @@ __global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __rest
         }
     }
     __syncthreads();
-    if (threadIdx.x < nv) {
+    if (threadIdx.x < kDotGroup && k0 + (int)threadIdx.x < nv) {
         double t = 0;
         for (int w8 = 0; w8 < 8; w8++) t += sh[w8][threadIdx.x];
-        G.partial[blockIdx.x * (kGmM + 1) + threadIdx.x] = t;
+        G.partial[blockIdx.x * (kGmM + 1) + k0 + threadIdx.x] = t;
     }
     if (gm_last_block(G)) {
         if (threadIdx.x < nv) {
@@ -241,7 +249,7 @@ void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* 
         precond_apply<VT>(A, P, z, done, st);
         spmv_skip<VT>(A, vals, z, w, done, st);
         k_gm_rowweight<VT><<<g, 256, 0, st>>>(n, w, rw, G);
-        k_gm_dots<VT><<<g, 256, 0, st>>>(n, j + 1, Vb, ld, j, G);
+        k_gm_dots<VT><<<dim3(g, (j + 1 + kDotGroup - 1) / kDotGroup), 256, 0, st>>>(n, j + 1, Vb, ld, j, G);
         k_gm_orth<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
         k_gm_scale<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
     }
