@@ -159,7 +159,15 @@ __global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ 
     double ss = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double v = w[i];
-        for (int k = 0; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
+        int k = 0;
+        for (; k + 8 <= j + 1; k += 8) {   // eight basis loads in flight, then the updates in order
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = (double)Vb[(size_t)(k + u) * ld + i];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v -= h[k + u] * x[u];
+        }
+        for (; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
         const VT vv = (VT)v;
         w[i] = vv;
         ss += (double)vv * (double)vv;
