@@ -37,6 +37,8 @@
  *        (selem_1d.c:86-125); see build_grid.
  *
  * Usage: adh_ref_harness <dump|run|time|mass> <case.bin> <out.bin> [every|reps]
+ *        adh_ref_harness init <case.bin> <out.bin> <init file base>
+ *        adh_ref_harness geo <grid.geo> <out.bin>
  *        adh_ref_harness rect - <out.bin> xmin xmax ymin ymax npx npy a0 ax
  */
 #include "adh.h"
@@ -392,6 +394,41 @@ static void mode_mass(const CASE *c) {
     out_rec("grid_mass", 'd', v, 4);
 }
 
+/* The reference's .geo reader, sgrid_read (src/structs/sgrid/sgrid_read.c:22), on a
+ * grid file: node coordinates, triangle and segment node ids (0-based) and triangle
+ * areas as the reader stores them.  argv = geo path, out path. */
+static void mode_geo(char **argv) {
+    SGRID *g = NULL;
+    sgrid_read(&g, argv[2]);
+    double *xyz = malloc(sizeof(double) * 3 * (g->nnodes + 1));
+    for (int i = 0; i < g->nnodes; i++) { xyz[3*i] = g->node[i].x; xyz[3*i+1] = g->node[i].y; xyz[3*i+2] = g->node[i].z; }
+    int *tri = malloc(sizeof(int) * 3 * (g->nelems2d + 1));
+    double *djac = malloc(sizeof(double) * (g->nelems2d + 1));
+    for (int e = 0; e < g->nelems2d; e++) {
+        for (int a = 0; a < 3; a++) tri[3*e+a] = g->elem2d[e].nodes[a];
+        djac[e] = g->elem2d[e].djac;
+    }
+    int *seg = malloc(sizeof(int) * 2 * (g->nelems1d + 1));
+    for (int e = 0; e < g->nelems1d; e++) { seg[2*e] = g->elem1d[e].nodes[0]; seg[2*e+1] = g->elem1d[e].nodes[1]; }
+    out_rec("xyz", 'd', xyz, 3 * (int64_t)g->nnodes);
+    out_rec("tri", 'i', tri, 3 * (int64_t)g->nelems2d);
+    out_rec("djac", 'd', djac, g->nelems2d);
+    out_rec("seg", 'i', seg, 2 * (int64_t)g->nelems1d);
+}
+
+/* The reference's .init reader, smodel_super_read_init (src/structs/smodel_super/
+ * smodel_super_read_init.c:26), on the case's model: the three solution levels start at
+ * zero as smodel_super_read allocates them (smodel_super_read.c), then the file's
+ * DATASETs fill them.  argv[4] = file base (the reader appends ".init"). */
+static void mode_init(char *filebase) {
+    SMODEL_SUPER *sm = g_sm;
+    for (int i = 0; i < sm->ndofs; i++) { sm->sol[i] = 0.; sm->sol_old[i] = 0.; sm->sol_older[i] = 0.; }
+    smodel_super_read_init(sm, filebase);
+    out_rec("sol", 'd', sm->sol, sm->ndofs);
+    out_rec("sol_old", 'd', sm->sol_old, sm->ndofs);
+    out_rec("sol_older", 'd', sm->sol_older, sm->ndofs);
+}
+
 /* The reference's own structured-grid generator (src/tools/create_rectangular_grid.c:4),
  * used to pin the flume mesh builder: argv = xmin xmax ymin ymax npx npy a0 ax. */
 static void mode_rect(int argc, char **argv) {
@@ -415,6 +452,16 @@ static void mode_rect(int argc, char **argv) {
 }
 
 int main(int argc, char **argv) {
+    if (argc >= 4 && strcmp(argv[1], "geo") == 0) {
+        if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
+        debug_initialize();
+        sadh_def_init();
+        g_out = fopen(argv[3], "wb");
+        if (!g_out) { fprintf(stderr, "harness: cannot write %s\n", argv[3]); return 2; }
+        mode_geo(argv);
+        fclose(g_out);
+        return 0;
+    }
     if (argc >= 4 && strcmp(argv[1], "rect") == 0) {
         if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
         debug_initialize();
@@ -440,6 +487,7 @@ int main(int argc, char **argv) {
     else if (strcmp(argv[1], "run") == 0) mode_run(&c, argc > 4 ? atoi(argv[4]) : 1);
     else if (strcmp(argv[1], "time") == 0) mode_time(&c, argc > 4 ? atoi(argv[4]) : 1);
     else if (strcmp(argv[1], "mass") == 0) mode_mass(&c);
+    else if (strcmp(argv[1], "init") == 0 && argc > 4) mode_init(argv[4]);
     else { fprintf(stderr, "harness: unknown mode %s\n", argv[1]); return 2; }
     fclose(g_out);
     return 0;

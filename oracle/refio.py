@@ -62,7 +62,8 @@ def read_records(path):
     return out
 
 
-def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=None, env=None, timeout=3600):
+def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=None, env=None, timeout=3600,
+                in_path=None):
     if not harness_available():
         raise RuntimeError("reference harness not built (oracle/_ref/adh_ref_harness)")
     with tempfile.TemporaryDirectory() as td:
@@ -70,13 +71,16 @@ def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=Non
         opath = os.path.join(td, "out.bin")
         if case is not None:
             write_case(case, cpath, sol, sol_old, sol_older)
+        elif in_path is not None:         # a mode that reads a file of its own (geo)
+            cpath = os.path.abspath(in_path)
         else:
             cpath = "-"
         e = dict(os.environ)
         if env:
             e.update(env)
+        # cwd: the reference's grid reader writes a node listing file into the working directory
         r = subprocess.run([HARNESS, mode, cpath, opath, *map(str, extra)], capture_output=True, env=e,
-                           timeout=timeout)
+                           timeout=timeout, cwd=td)
         if r.returncode != 0:
             raise RuntimeError(f"harness {mode} failed ({r.returncode}): {r.stderr.decode()[-2000:]}")
         return read_records(opath)
