@@ -208,10 +208,11 @@ __global__ void __launch_bounds__(256, kSweepBlocksPerSM) k_amg_l0(BlockCSR A, c
 }
 
 static int l0_grid(int nnodes, int lanes) { return grid_resident((long)nnodes * lanes, kSweepBlocksPerSM); }
-// lanes per node of the level-0 kernels, measured on the 4M beach (B200, 2M nodes, ~7 neighbours):
-// FP32 values 2 lanes (0.198 ms per sweep, 0.92 of the HBM copy peak) vs 4 (0.226) vs 8 (0.265);
-// FP64 4 lanes (0.304 ms) vs 8 (0.315).  Fewer lanes per node keep more independent loads in
-// flight per lane, which the latency-bound neighbour gathers need.
+// lanes per node of the level-0 kernels, measured on the 4M beach (B200, 2M nodes, ~7 neighbours)
+// with a grid of 8 blocks per SM: FP32 values 2 lanes (0.198 ms per sweep) vs 4 (0.226) vs 8
+// (0.265); FP64 4 lanes (0.304 ms) vs 8 (0.315).  Fewer lanes per node keep more independent
+// loads in flight per lane, which the latency-bound neighbour gathers need.  With the one-wave
+// grid (6 blocks per SM) the FP32 sweep takes 0.181 ms.
 template <class VT> struct L0Lanes { static constexpr int value = 4; };
 template <> struct L0Lanes<float> { static constexpr int value = 2; };
 
