@@ -88,7 +88,7 @@ def series_average(times, values, t1, t2):
 
 
 class OracleModel:
-    def __init__(self, case):
+    def __init__(self, case, tau_temporal=0.0):
         L = lib()
         self.case = case
         V, T, S = case.nnodes, case.ntri, case.nseg
@@ -109,7 +109,7 @@ class OracleModel:
         m.xyz, m.tri, m.seg, m.seg_kind = _d(self.xyz), _i(self.tri), _i(self.seg), _i(self.seg_kind)
         m.tri_djac, m.tri_grad, m.seg_djac, m.seg_nrml = _d(self.tri_djac), _d(self.tri_grad), _d(self.seg_djac), _d(self.seg_nrml)
         m.ndof, m.nnz, m.indptr, m.cols = 3 * V, nnz, _i(self.indptr), _i(self.cols)
-        m.gravity, m.dt, m.tau_temporal = case.gravity, case.dt, 0.0
+        m.gravity, m.dt, m.tau_temporal = case.gravity, case.dt, float(tau_temporal)
         m.wd_flag = _i(self.wd_flag)
         self.m = m
         self.ndof, self.nnz = 3 * V, nnz

@@ -233,7 +233,8 @@ static void build_model(const CASE *c) {
     sm->max_nonlin_it = c->max_nonlin_it;
     sm->gravity = c->gravity;
     g_dm.ts.dt = c->dt; g_dm.ts.t_prev = c->t0; g_dm.ts.t_init = c->t0; g_dm.ts.t_final = tf;
-    g_dm.ts.tau_temporal = 0.;
+    /* alpha of the three-level temporal scheme; the reference's default is 0 (sdt.c:24) */
+    g_dm.ts.tau_temporal = getenv("HARNESS_TAU") ? atof(getenv("HARNESS_TAU")) : 0.;
     for (int i = 0; i < sm->ndofs; i++) {
         sm->sol[i] = c->sol[i]; sm->sol_old[i] = c->sol_old[i]; sm->sol_older[i] = c->sol_older[i];
         sm->dirichlet_data[i] = 0.; sm->lin_sys->dsol[i] = 0.;

@@ -42,11 +42,12 @@ def case_arrays(case):
     return out
 
 
-def dump_fixture(name, case, seed):
+def dump_fixture(name, case, seed, tau=0.0):
     sol, sol_old, sol_older = perturbed_states(case, seed)
-    d = run_harness("dump", case, sol=sol, sol_old=sol_old, sol_older=sol_older)
+    env = {"HARNESS_TAU": repr(tau), "HARNESS_SKIP_SOLVE": "1"} if tau else None
+    d = run_harness("dump", case, sol=sol, sol_old=sol_old, sol_older=sol_older, env=env)
     arrs = case_arrays(case)
-    arrs.update({"sol": sol, "sol_old": sol_old, "sol_older": sol_older})
+    arrs.update({"sol": sol, "sol_old": sol_old, "sol_older": sol_older, "tau": tau})
     arrs.update({f"ref_{k}": v for k, v in d.items()})
     np.savez_compressed(os.path.join(HERE, name), **arrs)
 
@@ -95,6 +96,7 @@ def mass_fixture(name, case, seed, run_name=None):
 def main():
     dump_fixture("dump_flume_21x6.npz", flume_case(nsteps=1, npx=21, npy=6), seed=11)
     dump_fixture("dump_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=12)
+    dump_fixture("dump_wetdry_12_tau05.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=13, tau=0.5)
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
     run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)

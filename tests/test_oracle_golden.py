@@ -7,6 +7,12 @@ from fixtures import load, rel_err
 from oracle.oracle import OracleModel
 
 DUMPS = ["dump_flume_21x6.npz", "dump_wetdry_12.npz"]
+# the three-level temporal scheme (tau_temporal = 0.5; the reference's default is 0)
+DUMPS_TAU = DUMPS + ["dump_wetdry_12_tau05.npz"]
+
+
+def oracle_for(case, z):
+    return OracleModel(case, tau_temporal=float(z["tau"]) if "tau" in z.files else 0.0)
 RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz"]
 
 
@@ -27,10 +33,10 @@ def test_bc_series_average(name):
     assert np.array_equal(np.array(o.bc_values(case.t0, case.t0 + case.dt)), z["ref_bc_values"])
 
 
-@pytest.mark.parametrize("name", DUMPS)
+@pytest.mark.parametrize("name", DUMPS_TAU)
 def test_element_level_bit_exact(name):
     case, z = load(name)
-    o = OracleModel(case)
+    o = oracle_for(case, z)
     sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
     assert np.array_equal(o.wd_flags(sol, old), z["ref_wd_flag"])
     et, es = o.elem_resid(sol, old, older)
@@ -41,10 +47,10 @@ def test_element_level_bit_exact(name):
     assert np.array_equal(js, z["ref_elem_jac_seg"])
 
 
-@pytest.mark.parametrize("name", DUMPS)
+@pytest.mark.parametrize("name", DUMPS_TAU)
 def test_assembly_and_linear_system_bit_exact(name):
     case, z = load(name)
-    o = OracleModel(case)
+    o = oracle_for(case, z)
     sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
     o.wd_flags(sol, old)
     r = o.residual(sol, old, older)
