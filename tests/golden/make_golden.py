@@ -42,9 +42,23 @@ def case_arrays(case):
     return out
 
 
-def dump_fixture(name, case, seed, tau=0.0):
+def edge_depths(case, sol, seed):
+    """Put a sixth of the nodes at depths on the wet/dry boundary: exactly 0, -0,
+    +-1e-20 and 1e-300 (the current level only; the old level keeps the wet/dry flags
+    of the perturbed state)."""
+    rng = np.random.default_rng(seed)
+    nodes = rng.choice(case.nnodes, size=case.nnodes // 6, replace=False)
+    vals = np.array([0.0, -1e-20, 1e-20, 1e-300, -0.0])
+    sol = sol.copy()
+    sol[3 * nodes] = vals[np.arange(len(nodes)) % len(vals)]
+    return sol
+
+
+def dump_fixture(name, case, seed, tau=0.0, edge=False):
     sol, sol_old, sol_older = perturbed_states(case, seed)
-    env = {"HARNESS_TAU": repr(tau), "HARNESS_SKIP_SOLVE": "1"} if tau else None
+    if edge:
+        sol = edge_depths(case, sol, seed + 1)
+    env = {"HARNESS_TAU": repr(tau), "HARNESS_SKIP_SOLVE": "1"} if (tau or edge) else None
     d = run_harness("dump", case, sol=sol, sol_old=sol_old, sol_older=sol_older, env=env)
     arrs = case_arrays(case)
     arrs.update({"sol": sol, "sol_old": sol_old, "sol_older": sol_older, "tau": tau})
@@ -97,6 +111,7 @@ def main():
     dump_fixture("dump_flume_21x6.npz", flume_case(nsteps=1, npx=21, npy=6), seed=11)
     dump_fixture("dump_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=12)
     dump_fixture("dump_wetdry_12_tau05.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=13, tau=0.5)
+    dump_fixture("dump_wetdry_12_edge_depths.npz", small_delaunay_case(n=12, seed=5, nsteps=1), seed=17, edge=True)
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
     run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)

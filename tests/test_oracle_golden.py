@@ -7,8 +7,9 @@ from fixtures import load, rel_err
 from oracle.oracle import OracleModel
 
 DUMPS = ["dump_flume_21x6.npz", "dump_wetdry_12.npz"]
-# the three-level temporal scheme (tau_temporal = 0.5; the reference's default is 0)
-DUMPS_TAU = DUMPS + ["dump_wetdry_12_tau05.npz"]
+# the three-level temporal scheme (tau_temporal = 0.5; the reference's default is 0), and
+# depths on the wet/dry boundary (exactly 0, -0, +-1e-20, 1e-300) at a sixth of the nodes
+DUMPS_TAU = DUMPS + ["dump_wetdry_12_tau05.npz", "dump_wetdry_12_edge_depths.npz"]
 
 
 def oracle_for(case, z):
