@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from adh_kraken_b200.mesh import flume_case, small_delaunay_case, still_beach_case  # noqa: E402
+from adh_kraken_b200.mesh import basin_case, flume_case, small_delaunay_case, still_beach_case  # noqa: E402
 from oracle.refio import run_harness  # noqa: E402
 
 
@@ -115,6 +115,7 @@ def main():
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
     run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)
+    run_fixture("run_basin_12_6steps.npz", basin_case(n=12, seed=2, nsteps=6))
     mass_fixture("mass_flume_21x6.npz", flume_case(nsteps=8, npx=21, npy=6), 31, "run_flume_21x6_8steps.npz")
     mass_fixture("mass_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=4), 41, "run_wetdry_12_4steps.npz")
     for f in sorted(os.listdir(HERE)):

@@ -14,7 +14,8 @@ DUMPS_TAU = DUMPS + ["dump_wetdry_12_tau05.npz", "dump_wetdry_12_edge_depths.npz
 
 def oracle_for(case, z):
     return OracleModel(case, tau_temporal=float(z["tau"]) if "tau" in z.files else 0.0)
-RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz"]
+RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz",
+        "run_basin_12_6steps.npz"]   # tidal depth boundary, a 1 m / 12.42 h sine series
 
 
 @pytest.mark.parametrize("name", DUMPS)
@@ -95,6 +96,17 @@ def test_time_steps_match_reference(name):
     assert all(h["ok"] for h in hist)
     ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
     assert max(rel_err(sol, ref)) < 1e-8
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_step_averaged_series_every_step(name):
+    """sseries_setall_ts_valuesAVG over each step's [t - dt, t], bit for bit, on every
+    step of the runs (the basin's tide has four samples per step)."""
+    case, z = load(name)
+    o = OracleModel(case)
+    n = len(z["ref_step_ok"])
+    mine = [o.bc_values(case.t0 + k * case.dt, case.t0 + (k + 1) * case.dt) for k in range(n)]
+    assert np.array_equal(np.array(mine).ravel(), z["ref_bc_values"])
 
 
 MASS = ["mass_flume_21x6.npz", "mass_wetdry_12.npz"]
