@@ -35,3 +35,22 @@ def test_default_options_match_reference_defaults():
     # bcgstab_solver.c:20-21 tolerance 1e-11
     assert (o.tol_nonlin, o.inc_nonlin, o.max_nonlin_it, o.max_linesearch_cuts) == (1e-8, 1e-6, 10, 5)
     assert o.krylov_tol == 1e-11 and o.krylov_precision == 64 and o.use_guess == 0
+
+
+def test_headers_compile_as_c99_and_cxx(tmp_path):
+    """The reference is C99: both headers must compile in a C99 and a C++ unit as the
+    reference-side caller would include them."""
+    import shutil
+    import subprocess
+    import pytest
+    src = tmp_path / "use.c"
+    src.write_text('#include "adh_sw2_gpu.h"\n#include "adh_sw2_gnn.h"\n'
+                   "int use(sw2g_model *m) { double out[2]; return sw2g_grid_mass(m, 0, 1.0, 1.0, out, 0); }\n")
+    inc = os.path.join(ROOT, "include")
+    for cc, std in (("gcc", "-std=c99"), ("g++", "-std=c++17")):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not available")
+        lang = ["-x", "c++"] if cc == "g++" else []
+        r = subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror", "-pedantic", "-fsyntax-only", "-I", inc,
+                            *lang, str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
