@@ -1,0 +1,135 @@
+"""Node partition, split CSR and halo plan for running the SW2 linear algebra on
+several ranks, and the distributed matrix-vector product and dot product over
+torch.distributed (gloo on CPU here; the same plan serves NCCL ranks).
+
+The layout restates the reference's distributed design:
+
+* nodes split into contiguous ranges, ``npes`` ranges of ``nnodes // npes`` nodes
+  with the remainder on the last rank (node_ind_ptr, src/structs/sgrid/sgrid_read.c:172-178);
+* each rank owns the dofs of its nodes and holds a split CSR
+  (src/structs/slin_sys/slin_sys.h:13-22): a diagonal block whose columns are local
+  dof numbers, and an off-diagonal block whose columns are global dof numbers of
+  ghost dofs, resolved through the rank's ``ghosts`` list (local number =
+  nrows + position in ghosts, global_to_local);
+* y = A x row by row, the diagonal block's entries first and then the off-diagonal
+  block's, each in column order (split_CSR_mat_vec_mult, src/la/matrix_utilities.c:177-215).
+
+The ghost values come from their owners before each product (the halo exchange the
+reference leaves stubbed at src/la/bcgstab_solver.c:152-158).  Ghost dofs are kept in
+increasing global order.  Host code: the arrays are numpy, the exchange is
+torch.distributed point-to-point on CPU tensors.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, List
+
+import numpy as np
+
+
+def node_ranges(nnodes: int, npes: int) -> np.ndarray:
+    """node_ind_ptr: rank r owns nodes [ptr[r], ptr[r+1])."""
+    per = nnodes // npes
+    ptr = np.arange(npes + 1, dtype=np.int64) * per
+    ptr[npes] = nnodes
+    return ptr
+
+
+@dataclass
+class RankCSR:
+    rank: int
+    row0: int                      # first owned global dof
+    nrows: int                     # owned dofs
+    indptr_diag: np.ndarray
+    cols_diag: np.ndarray          # local dof numbers
+    vals_diag: np.ndarray
+    indptr_off: np.ndarray
+    cols_off: np.ndarray           # global dof numbers (ghosts)
+    vals_off: np.ndarray
+    ghosts: np.ndarray             # sorted global dof numbers of the ghost dofs
+    send: Dict[int, np.ndarray] = field(default_factory=dict)   # peer -> owned global dofs the peer needs
+    recv: Dict[int, np.ndarray] = field(default_factory=dict)   # peer -> positions in ghosts it fills
+
+
+def split(indptr: np.ndarray, cols: np.ndarray, vals: np.ndarray, nnodes: int, npes: int) -> List[RankCSR]:
+    """Every rank's split CSR of the global CSR (dof = 3 node + var) and the halo plan."""
+    ptr = node_ranges(nnodes, npes)
+    dof_ptr = 3 * ptr
+    out = []
+    for r in range(npes):
+        r0, r1 = int(dof_ptr[r]), int(dof_ptr[r + 1])
+        ip_d, c_d, v_d, ip_o, c_o, v_o = [0], [], [], [0], [], []
+        for row in range(r0, r1):
+            k0, k1 = int(indptr[row]), int(indptr[row + 1])
+            c, v = cols[k0:k1], vals[k0:k1]
+            own = (c >= r0) & (c < r1)
+            c_d.append(c[own] - r0); v_d.append(v[own])
+            c_o.append(c[~own]); v_o.append(v[~own])
+            ip_d.append(ip_d[-1] + int(own.sum())); ip_o.append(ip_o[-1] + int((~own).sum()))
+        cat = lambda a, dt: np.concatenate(a).astype(dt) if a else np.zeros(0, dt)   # noqa: E731
+        cols_off = cat(c_o, np.int64)
+        ghosts = np.unique(cols_off)
+        out.append(RankCSR(r, r0, r1 - r0, np.array(ip_d, np.int64), cat(c_d, np.int64), cat(v_d, vals.dtype),
+                           np.array(ip_o, np.int64), cols_off, cat(v_o, vals.dtype), ghosts))
+    owner = lambda g: int(np.searchsorted(dof_ptr, g, side="right") - 1)   # noqa: E731
+    for p in out:
+        if p.ghosts.size == 0:
+            continue
+        owners = np.array([owner(g) for g in p.ghosts])
+        for q in np.unique(owners):
+            sel = np.nonzero(owners == q)[0]
+            p.recv[int(q)] = sel
+            out[int(q)].send[p.rank] = p.ghosts[sel]
+    return out
+
+
+def local_index(p: RankCSR, g: np.ndarray) -> np.ndarray:
+    """global_to_local for ghost dofs: nrows + position in the ghost list."""
+    return p.nrows + np.searchsorted(p.ghosts, g)
+
+
+def matvec_local(p: RankCSR, x_ext: np.ndarray) -> np.ndarray:
+    """split_CSR_mat_vec_mult on one rank: x_ext = owned values then ghost values."""
+    y = np.zeros(p.nrows, dtype=x_ext.dtype)
+    off_local = local_index(p, p.cols_off)
+    for i in range(p.nrows):
+        s = 0.0
+        for j in range(p.indptr_diag[i], p.indptr_diag[i + 1]):
+            s += p.vals_diag[j] * x_ext[p.cols_diag[j]]
+        for k in range(p.indptr_off[i], p.indptr_off[i + 1]):
+            s += p.vals_off[k] * x_ext[off_local[k]]
+        y[i] = s
+    return y
+
+
+def halo_exchange(p: RankCSR, x_own: np.ndarray, dist) -> np.ndarray:
+    """Owned values plus the ghost values received from their owners (point-to-point,
+    every pair in the same order on both sides)."""
+    import torch
+    x_ext = np.concatenate([x_own, np.zeros(p.ghosts.size, x_own.dtype)])
+    reqs, bufs = [], {}
+    for q, dofs in sorted(p.send.items()):
+        t = torch.from_numpy(np.ascontiguousarray(x_own[dofs - p.row0]))
+        reqs.append(dist.isend(t, dst=q))
+        bufs[("s", q)] = t
+    for q, pos in sorted(p.recv.items()):
+        t = torch.empty(len(pos), dtype=torch.float64 if x_own.dtype == np.float64 else torch.float32)
+        reqs.append(dist.irecv(t, src=q))
+        bufs[("r", q)] = t
+    for rq in reqs:
+        rq.wait()
+    for q, pos in p.recv.items():
+        x_ext[p.nrows + pos] = bufs[("r", q)].numpy()
+    return x_ext
+
+
+def matvec(p: RankCSR, x_own: np.ndarray, dist) -> np.ndarray:
+    return matvec_local(p, halo_exchange(p, x_own, dist))
+
+
+def dot(a_own: np.ndarray, b_own: np.ndarray, dist) -> float:
+    """Global dot product: local sums, then one all-reduce (messg_dsum)."""
+    import torch
+    t = torch.tensor([float(np.dot(a_own, b_own))], dtype=torch.float64)
+    dist.all_reduce(t)
+    return float(t.item())

@@ -1,0 +1,102 @@
+"""The multi-rank plumbing of the linear algebra on CPU: node partition, split CSR,
+halo plan, and the distributed matrix-vector and dot products over gloo ranks
+(world size 2 and 3) against the single-process product."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from adh_kraken_b200.mesh import small_delaunay_case
+from adh_kraken_b200.partition import matvec_local, node_ranges, split
+from oracle.oracle import OracleModel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def system(seed=0):
+    case = small_delaunay_case(n=12, seed=5, nsteps=1)
+    o = OracleModel(case)
+    rng = np.random.default_rng(seed)
+    vals = rng.standard_normal(o.nnz)
+    x = rng.standard_normal(o.ndof)
+    return case, o, vals, x
+
+
+def emulate(parts, x):
+    """Every rank's product with its ghost values taken straight from x."""
+    out = []
+    for p in parts:
+        x_ext = np.concatenate([x[p.row0:p.row0 + p.nrows], x[p.ghosts]])
+        out.append(matvec_local(p, x_ext))
+    return np.concatenate(out)
+
+
+def test_node_ranges_follow_the_reference_split():
+    assert node_ranges(10, 3).tolist() == [0, 3, 6, 10]      # nnodes / npes each, the rest on the last
+    assert node_ranges(7, 1).tolist() == [0, 7]
+
+
+@pytest.mark.parametrize("npes", [1, 2, 3])
+def test_split_csr_and_halo_plan(npes):
+    case, o, vals, x = system()
+    parts = split(o.indptr, o.cols, vals, case.nnodes, npes)
+    assert sum(p.nrows for p in parts) == o.ndof
+    assert sum(p.cols_diag.size + p.cols_off.size for p in parts) == o.nnz
+    for p in parts:
+        own = (p.ghosts >= p.row0) & (p.ghosts < p.row0 + p.nrows)
+        assert not own.any()
+        for q, pos in p.recv.items():
+            assert np.array_equal(parts[q].send[p.rank], p.ghosts[pos])
+        assert sorted(np.concatenate(list(p.recv.values())).tolist() if p.recv else []) == list(range(p.ghosts.size))
+    y = emulate(parts, x)
+    ref = o.spmv(vals, x)
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+    if npes == 1:
+        assert np.array_equal(y, ref)      # one rank: the diagonal block is the whole row, same order
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from adh_kraken_b200.partition import dot, matvec, split as split_
+    case, o, vals, x = system()
+    p = split_(o.indptr, o.cols, vals, case.nnodes, world)[rank]
+    own = x[p.row0:p.row0 + p.nrows]
+    y = matvec(p, own, dist)
+    d = dot(own, own, dist)
+    out[rank] = (p.row0, y, d)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_matvec_and_dot_over_gloo(world):
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    case, o, vals, x = system()
+    parts = split(o.indptr, o.cols, vals, case.nnodes, world)
+    y = np.concatenate([out[r][1] for r in range(world)])
+    assert np.array_equal(y, emulate(parts, x))          # the exchanged ghosts are the owners' values
+    assert all(abs(out[r][2] - float(np.dot(x, x))) <= 1e-12 * float(np.dot(x, x)) for r in range(world))
