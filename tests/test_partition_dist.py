@@ -100,3 +100,50 @@ def test_distributed_matvec_and_dot_over_gloo(world):
     y = np.concatenate([out[r][1] for r in range(world)])
     assert np.array_equal(y, emulate(parts, x))          # the exchanged ghosts are the owners' values
     assert all(abs(out[r][2] - float(np.dot(x, x))) <= 1e-12 * float(np.dot(x, x)) for r in range(world))
+
+
+def _bicg_worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from fixtures import load
+    from adh_kraken_b200.partition import bicgstab_bj, split as split_
+    case, z = load("dump_wetdry_12.npz")
+    o = OracleModel(case)
+    p = split_(o.indptr, o.cols, z["ref_jac_vals_scaled"], case.nnodes, world)[rank]
+    sl = slice(p.row0, p.row0 + p.nrows)
+    x, it = bicgstab_bj(p, np.zeros(p.nrows), z["ref_residual_scaled"][sl].copy(), z["ref_scale_vect"][sl], dist,
+                        max_it=20000, tol=1e-13)
+    out[rank] = (x, it)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_distributed_block_jacobi_bicgstab_matches_the_single_process_solve():
+    """The reference's BiCGStab recurrence on two ranks (halo exchange per product,
+    all-reduce per dot and max-norm) against the oracle's single-process solve of the
+    same scaled system from the reference's dump."""
+    from fixtures import load
+    world = 2
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_bicg_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(180)
+    assert all(p.exitcode == 0 for p in procs)
+    case, z = load("dump_wetdry_12.npz")
+    o = OracleModel(case)
+    v = z["ref_jac_vals_scaled"].copy(); b = z["ref_residual_scaled"].copy(); x1 = np.zeros(o.ndof)
+    it1 = o.bicgstab(v, x1, b, z["ref_scale_vect"], max_it=20000, tol=1e-13)
+    xd = np.concatenate([out[r][0] for r in range(world)])
+    its = {out[r][1] for r in range(world)}
+    assert len(its) == 1 and it1 > 0 and abs(its.pop() - it1) <= 2
+    assert np.abs(xd - x1).max() <= 1e-9 * np.abs(x1).max()
+    assert np.abs(xd - z["ref_dsol"]).max() <= 1e-6 * np.abs(z["ref_dsol"]).max()
