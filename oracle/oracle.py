@@ -189,11 +189,12 @@ class OracleModel:
 
     def newton(self, sol, sol_old, sol_older, bc_mask, dirichlet, krylov_max_it=100, krylov_tol=1e-11):
         c = self.case
-        stats = np.zeros(4)
+        stats = np.zeros(5)
         lib().sw2o_newton(C.byref(self.m), _d(sol), _d(sol_old), _d(sol_older), _i(bc_mask), _d(dirichlet),
                           C.c_double(c.tol_nonlin), C.c_double(c.inc_nonlin), c.max_nonlin_it, 5, krylov_max_it,
                           C.c_double(krylov_tol), _d(stats))
-        return {"newton_its": int(stats[0]), "krylov_its": int(stats[1]), "resid_max": stats[2], "ok": bool(stats[3])}
+        return {"newton_its": int(stats[0]), "krylov_its": int(stats[1]), "resid_max": stats[2], "ok": bool(stats[3]),
+                "linesearch_cuts": int(stats[4])}
 
     def run(self, nsteps=None, krylov_max_it=100, krylov_tol=1e-11):
         """Time loop of src/timeloop/time_loop.c:14-89: rotate levels, average the

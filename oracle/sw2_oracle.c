@@ -858,7 +858,7 @@ int sw2o_newton(sw2o_model *m, double *sol, const double *sol_old, const double 
     sw2o_assemble_residual(m, sol, sol_old, sol_older, res);
     double rmax, rl2, imax, old_l2;
     resid_norms(n, res, dsol, bc_mask, &rmax, &rl2, &imax);
-    int it = 0, kry_total = 0, ok = 1, keep;
+    int it = 0, kry_total = 0, cuts_total = 0, ok = 1, keep;
     do {
         sw2o_assemble_jacobian(m, sol, sol_old, sol_older, vals);
         sw2o_check_diag(m, vals, bc_mask);
@@ -881,11 +881,19 @@ int sw2o_newton(sw2o_model *m, double *sol, const double *sol_old, const double 
             resid_norms(n, res, dsol, bc_mask, &rmax, &rl2, &imax);
             cuts++;
         }
+        cuts_total += cuts;
         it++;
         keep = ok && it < max_nonlin_it && rmax < 1.0E+20 && rmax > tol_nonlin && imax > inc_nonlin;
     } while (keep);
     int success = !(((rmax > tol_nonlin) && (imax > inc_nonlin)) || (rmax >= 1.0E+20) || !ok);
-    stats[0] = it; stats[1] = kry_total; stats[2] = rmax; stats[3] = success;
+    if (!success) {   /* fe_newton.c:893-899: initialize_system, then initialize_dirichlet_bc */
+        memcpy(sol, sol_old, 8 * (size_t)n);
+        sw2o_wd_flags(m, sol, sol_old);
+        for (int i = 0; i < m->nnodes; i++)
+            if (sol_old[3 * i] <= 0.) { bc_mask[3 * i + 1] = 1; bc_mask[3 * i + 2] = 1; }
+        for (int i = 0; i < n; i++) if (bc_mask[i] == 1) sol[i] = dirichlet[i];
+    }
+    stats[0] = it; stats[1] = kry_total; stats[2] = rmax; stats[3] = success; stats[4] = cuts_total;
     free(res); free(dsol); free(vals); free(sv);
     return success;
 }

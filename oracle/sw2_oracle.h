@@ -81,10 +81,12 @@ int sw2o_bicgstab_bj(int n, const int *indptr, const int *cols, const double *va
                      double *b, const double *scale_vect, int max_it, double tol);
 
 /* fe_newton (src/newton/fe_newton.c:44) for one time step with block-Jacobi BiCGStab.
- * On entry sol_old/sol_older hold the previous levels; sol receives the result.
+ * On entry sol_old/sol_older hold the previous levels; sol receives the result (on
+ * failure, the start of the step again, as fe_newton resets it).
  * bc_mask (ndof) and dirichlet (ndof) persist across steps like sm->bc_mask.
  * stats[0] = Newton iterations, stats[1] = total Krylov iterations,
- * stats[2] = final residual max norm, stats[3] = success flag. */
+ * stats[2] = final residual max norm, stats[3] = success flag, stats[4] = line-search
+ * halvings over all Newton iterations. */
 int sw2o_newton(sw2o_model *m, double *sol, const double *sol_old, const double *sol_older,
                 int *bc_mask, const double *dirichlet, double tol_nonlin, double inc_nonlin,
                 int max_nonlin_it, int max_linesearch_cuts, int krylov_max_it, double krylov_tol,

@@ -116,6 +116,9 @@ def main():
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
     run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)
     run_fixture("run_basin_12_6steps.npz", basin_case(n=12, seed=2, nsteps=6))
+    # dt 600 s: four line-search halvings in the first Newton solve; dt 150 s: a failed solve
+    run_fixture("run_wetdry_12_dt600_6steps.npz", small_delaunay_case(n=12, seed=5, nsteps=6, dt=600.0))
+    run_fixture("run_wetdry_12_dt150_fail.npz", small_delaunay_case(n=12, seed=5, nsteps=3, dt=150.0))
     mass_fixture("mass_flume_21x6.npz", flume_case(nsteps=8, npx=21, npy=6), 31, "run_flume_21x6_8steps.npz")
     mass_fixture("mass_wetdry_12.npz", small_delaunay_case(n=12, seed=5, nsteps=4), 41, "run_wetdry_12_4steps.npz")
     for f in sorted(os.listdir(HERE)):

@@ -15,7 +15,8 @@ DUMPS_TAU = DUMPS + ["dump_wetdry_12_tau05.npz", "dump_wetdry_12_edge_depths.npz
 def oracle_for(case, z):
     return OracleModel(case, tau_temporal=float(z["tau"]) if "tau" in z.files else 0.0)
 RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz",
-        "run_basin_12_6steps.npz"]   # tidal depth boundary, a 1 m / 12.42 h sine series
+        "run_basin_12_6steps.npz",          # tidal depth boundary, a 1 m / 12.42 h sine series
+        "run_wetdry_12_dt600_6steps.npz"]   # line-search halvings in the first solve
 
 
 @pytest.mark.parametrize("name", DUMPS)
@@ -107,6 +108,31 @@ def test_step_averaged_series_every_step(name):
     n = len(z["ref_step_ok"])
     mine = [o.bc_values(case.t0 + k * case.dt, case.t0 + (k + 1) * case.dt) for k in range(n)]
     assert np.array_equal(np.array(mine).ravel(), z["ref_bc_values"])
+
+
+def test_line_search_is_exercised():
+    """The dt = 600 s run halves its first Newton increments (fe_newton.c:681-741)
+    and still lands on the reference's states (test_time_steps_match_reference)."""
+    case, z = load("run_wetdry_12_dt600_6steps.npz")
+    o = OracleModel(case)
+    _, hist = o.run(2, krylov_max_it=20000)
+    assert hist[0]["linesearch_cuts"] >= 3 and hist[0]["newton_its"] == int(z["ref_newton_its"][0])
+
+
+def test_failed_newton_solve_resets_like_the_reference():
+    """dt = 150 s: the first solve fails after max_nonlin_it iterations in the
+    reference as in the oracle; both reset the state to the start of the step with the
+    Dirichlet values and the dry-node marks (fe_newton.c:893-899), bit for bit."""
+    case, z = load("run_wetdry_12_dt150_fail.npz")
+    assert z["ref_step_ok"].tolist() == [0]
+    o = OracleModel(case)
+    sol = case.sol0.copy(); old = sol.copy(); older = sol.copy()
+    bc = np.zeros(o.ndof, np.int32)
+    o.set_bc_window(case.t0, case.t0 + case.dt)
+    st = o.newton(sol, old, older, bc, np.zeros(o.ndof), krylov_max_it=20000)
+    assert not st["ok"] and st["newton_its"] == int(z["ref_newton_its"][0])
+    assert np.array_equal(sol, z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1])
+    assert np.array_equal(bc, (z["ref_bc_mask"] == 1).astype(np.int32))
 
 
 MASS = ["mass_flume_21x6.npz", "mass_wetdry_12.npz"]
