@@ -54,3 +54,16 @@ def test_headers_compile_as_c99_and_cxx(tmp_path):
         r = subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror", "-pedantic", "-fsyntax-only", "-I", inc,
                             *lang, str(src)], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_no_cpu_fallback_without_a_gpu():
+    """Without a usable GPU the model constructor fails with the CUDA error; nothing
+    falls back to a CPU path."""
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from adh_kraken_b200.capi import SW2Error, SW2Model
+    from adh_kraken_b200.mesh import small_delaunay_case
+    with pytest.raises(SW2Error, match="cuda|CUDA"):
+        SW2Model(small_delaunay_case(n=12, seed=5))
