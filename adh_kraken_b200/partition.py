@@ -226,3 +226,97 @@ def bicgstab_bj(p: RankCSR, x_own: np.ndarray, b_own: np.ndarray, scale_own: np.
             break
     x = (x + x0) * scale_own
     return x, (-it - 1 if status < 0 else it)
+
+
+# ---------------------------------------------------------------------------- assembly
+@dataclass
+class AssemblyPart:
+    """What one rank needs to assemble its own rows without exchanging element
+    contributions: every triangle within two element rings of its nodes (the
+    wet/dry flag of an element next to an owned node depends on the elements around
+    that element's nodes), the boundary segments that touch its nodes, and the nodes
+    all of them reference.  Elements keep their global order and nodes their global
+    order, so each owned row sums the same element contributions in the same order
+    as the single-process assembly."""
+    rank: int
+    lo: int
+    hi: int
+    tri_ids: np.ndarray     # global triangle ids, increasing
+    seg_ids: np.ndarray     # global segment ids, increasing
+    nodes: np.ndarray       # global node ids, increasing (local node k = nodes[k])
+
+    def local(self, g: np.ndarray) -> np.ndarray:
+        return np.searchsorted(self.nodes, g)
+
+    @property
+    def owned_local(self) -> np.ndarray:
+        return self.local(np.arange(self.lo, self.hi))
+
+
+def assembly_parts(tri: np.ndarray, seg: np.ndarray, nnodes: int, npes: int) -> List[AssemblyPart]:
+    ptr = node_ranges(nnodes, npes)
+    out = []
+    for r in range(npes):
+        lo, hi = int(ptr[r]), int(ptr[r + 1])
+        owned = np.zeros(nnodes, bool)
+        owned[lo:hi] = True
+        ring1 = owned[tri].any(axis=1)
+        n1 = np.zeros(nnodes, bool)
+        n1[tri[ring1].ravel()] = True
+        n1 |= owned
+        ring2 = n1[tri].any(axis=1)
+        sg = owned[seg].any(axis=1) if seg.size else np.zeros(0, bool)
+        nodes = np.unique(np.concatenate([tri[ring2].ravel(), seg[sg].ravel(), np.arange(lo, hi)]))
+        out.append(AssemblyPart(r, lo, hi, np.nonzero(ring2)[0], np.nonzero(sg)[0], nodes))
+    return out
+
+
+def part_case(case, part: AssemblyPart):
+    """The rank's sub-mesh as a case in local numbering (same forcing and step)."""
+    import dataclasses
+    loc = part.local
+    tri = loc(case.tri[part.tri_ids]).astype(np.int32)
+    seg = loc(case.seg[part.seg_ids]).astype(np.int32).reshape(-1, 2)
+    dofs = (3 * part.nodes[:, None] + np.arange(3)).ravel()
+    return dataclasses.replace(case, xyz=case.xyz[part.nodes], tri=tri, seg=seg,
+                               seg_kind=case.seg_kind[part.seg_ids], sol0=case.sol0[dofs]), dofs
+
+
+def state_halo(parts: List[AssemblyPart], nnodes: int):
+    """For each rank: {peer: global nodes it receives from that peer} and
+    {peer: global nodes it sends}, node-wise (three dofs per node)."""
+    ptr = node_ranges(nnodes, len(parts))
+    recv = [dict() for _ in parts]
+    send = [dict() for _ in parts]
+    for p in parts:
+        ghost = p.nodes[(p.nodes < p.lo) | (p.nodes >= p.hi)]
+        owner = np.searchsorted(ptr, ghost, side="right") - 1
+        for q in np.unique(owner):
+            g = ghost[owner == q]
+            recv[p.rank][int(q)] = g
+            send[int(q)][p.rank] = g
+    return send, recv
+
+
+def exchange_state(part: AssemblyPart, send: Dict[int, np.ndarray], recv: Dict[int, np.ndarray],
+                   state_own: np.ndarray, dist) -> np.ndarray:
+    """This rank's state vector in the part's local node order: owned nodes from
+    state_own (3 values per owned node), the others from their owners."""
+    import torch
+    out = np.zeros(3 * part.nodes.size, dtype=state_own.dtype)
+    own = part.owned_local
+    out.reshape(-1, 3)[own] = state_own.reshape(-1, 3)
+    reqs, bufs = [], {}
+    for q, g in sorted(send.items()):
+        t = torch.from_numpy(np.ascontiguousarray(state_own.reshape(-1, 3)[g - part.lo].ravel()))
+        reqs.append(dist.isend(t, dst=q))
+        bufs[("s", q)] = t
+    for q, g in sorted(recv.items()):
+        t = torch.empty(3 * g.size, dtype=torch.float64)
+        reqs.append(dist.irecv(t, src=q))
+        bufs[("r", q)] = t
+    for rq in reqs:
+        rq.wait()
+    for q, g in recv.items():
+        out.reshape(-1, 3)[part.local(g)] = bufs[("r", q)].numpy().reshape(-1, 3)
+    return out
