@@ -320,3 +320,133 @@ def exchange_state(part: AssemblyPart, send: Dict[int, np.ndarray], recv: Dict[i
     for q, g in recv.items():
         out.reshape(-1, 3)[part.local(g)] = bufs[("r", q)].numpy().reshape(-1, 3)
     return out
+
+
+# ---------------------------------------------------------------------------- Newton
+def _gsum(v: float, dist) -> float:
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64)
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+class RankNewton:
+    """fe_newton (src/newton/fe_newton.c:44-915) for one rank of a partitioned run:
+    residual and Jacobian rows from the rank's halo sub-mesh (``make_model`` builds
+    the element evaluator for it: an object with wd_flags / residual / jacobian on
+    local states, such as the CPU oracle or a device model), check_diag, Dirichlet
+    rows and columns, row and column scaling, block-Jacobi BiCGStab over the split
+    CSR, the line search and the stop tests, with the norms and dot products reduced
+    over the ranks.  Column operations read the ghost columns' Dirichlet marks and
+    scale factors through the same halo as the products."""
+
+    SMALL = float(np.finfo(np.float64).eps)
+
+    def __init__(self, case, indptr, cols, npes, rank, make_model):
+        self.case, self.npes, self.rank = case, npes, rank
+        parts = assembly_parts(case.tri, case.seg, case.nnodes, npes)
+        self.part = parts[rank]
+        self.send, self.recv = state_halo(parts, case.nnodes)
+        self.send, self.recv = self.send[rank], self.recv[rank]
+        sub, _ = part_case(case, self.part)
+        self.model = make_model(sub)
+        self.plan = split(indptr, cols, np.zeros(len(cols)), case.nnodes, npes)[rank]
+        self.r0, self.r1 = 3 * self.part.lo, 3 * self.part.hi
+        rows = slice(int(indptr[self.r0]), int(indptr[self.r1]))
+        self.row_cols = np.asarray(cols[rows], np.int64)
+        self.row_ptr = np.asarray(indptr[self.r0:self.r1 + 1], np.int64) - int(indptr[self.r0])
+        self.diag_mask = (self.row_cols >= self.r0) & (self.row_cols < self.r1)
+        self.own_rows = (3 * self.part.owned_local[:, None] + np.arange(3)).ravel()
+        row_of = np.repeat(np.arange(self.r1 - self.r0), np.diff(self.row_ptr))
+        self.diag_slot = np.nonzero(self.row_cols == row_of + self.r0)[0]
+        self.n_global = 3 * case.nnodes
+
+    # -- helpers
+    def _local(self, sol_own, dist):
+        return exchange_state(self.part, self.send, self.recv, sol_own, dist)
+
+    def _ghost_values(self, v_own, dist):
+        return halo_exchange(self.plan, v_own, dist)[self.plan.nrows:]
+
+    def _col_values(self, v_own, v_ghost):
+        """v at every matrix entry's column (owned columns from v_own, ghosts from v_ghost)."""
+        out = np.empty(self.row_cols.size)
+        out[self.diag_mask] = v_own[self.row_cols[self.diag_mask] - self.r0]
+        out[~self.diag_mask] = v_ghost[np.searchsorted(self.plan.ghosts, self.row_cols[~self.diag_mask])]
+        return out
+
+    def _residual(self, sol_own, old_loc, older_loc, dist):
+        r = self.model.residual(self._local(sol_own, dist), old_loc, older_loc)
+        return r[self.own_rows]
+
+    def _jacobian(self, sol_own, old_loc, older_loc, dist):
+        v = self.model.jacobian(self._local(sol_own, dist), old_loc, older_loc)
+        ip = self.model.indptr
+        return np.concatenate([v[ip[r]:ip[r + 1]] for r in self.own_rows])
+
+    def _norms(self, res, dsol, mask, dist):
+        inc = mask != 1
+        rmax = _gmax(res[inc], dist) if True else 0.0
+        l2 = _gsum(float(np.sum(res[inc] * res[inc])), dist)
+        imax = _gmax(dsol[inc], dist)
+        return rmax, np.sqrt(l2) / self.n_global, imax
+
+    def solve(self, sol_old_own, sol_older_own, mask_own, dirichlet_own, dist, tol_nonlin=1e-8, inc_nonlin=1e-6,
+              max_nonlin_it=10, max_cuts=5, krylov_max_it=100, krylov_tol=1e-11):
+        old_loc = self._local(sol_old_own, dist)
+        older_loc = self._local(sol_older_own, dist)
+        n = self.r1 - self.r0
+        # initialize_system (newton_tools.c:21-37) and fe_sw2_init's dry-node marks
+        sol = sol_old_own.copy()
+        self.model.wd_flags(self._local(sol, dist), old_loc)
+        dry = np.nonzero(sol_old_own[0::3] <= 0.0)[0]
+        mask_own[3 * dry + 1] = 1
+        mask_own[3 * dry + 2] = 1
+        sol[mask_own == 1] = dirichlet_own[mask_own == 1]
+        res = self._residual(sol, old_loc, older_loc, dist)
+        dsol = np.zeros(n)
+        rmax, rl2, imax = self._norms(res, dsol, mask_own, dist)
+        it, kry, ok, cuts_total = 0, 0, True, 0
+        while True:
+            vals = self._jacobian(sol, old_loc, older_loc, dist)
+            mask_own[np.abs(vals[self.diag_slot]) < self.SMALL] = 1                 # check_diag
+            mask_col = self._col_values(mask_own.astype(np.float64), self._ghost_values(mask_own.astype(np.float64), dist))
+            vals[mask_col == 1.0] = 0.0                                                # Dirichlet columns
+            for r in np.nonzero(mask_own == 1)[0]:                                     # Dirichlet rows
+                k0, k1 = self.row_ptr[r], self.row_ptr[r + 1]
+                vals[k0:k1] = (self.row_cols[k0:k1] == r + self.r0).astype(np.float64)
+                res[r] = 0.0
+            mx = np.array([np.max(np.abs(vals[self.row_ptr[r]:self.row_ptr[r + 1]])) for r in range(n)])
+            s = np.where(mx < self.SMALL, 1.0 / np.sqrt(self.SMALL), 1.0 / np.sqrt(np.abs(mx)))
+            b = res * s
+            s_col = self._col_values(s, self._ghost_values(s, dist))
+            row_of = np.repeat(np.arange(n), np.diff(self.row_ptr))
+            vals = vals * (s[row_of] * s_col)
+            p = self.plan
+            p.vals_diag, p.vals_off = vals[self.diag_mask], vals[~self.diag_mask]
+            dsol, kit = bicgstab_bj(p, np.zeros(n), b, s, dist, max_it=krylov_max_it, tol=krylov_tol)
+            kry += kit if kit >= 0 else -kit - 1
+            sol = sol + dsol
+            dsol = -dsol
+            old_l2 = rl2
+            res = self._residual(sol, old_loc, older_loc, dist)
+            rmax, rl2, imax = self._norms(res, dsol, mask_own, dist)
+            if not np.isfinite(rl2):
+                ok = False
+            cuts = 0
+            while rmax > tol_nonlin and rl2 > old_l2 and cuts < max_cuts:              # line search
+                dsol = dsol * 0.5
+                sol = sol + dsol
+                res = self._residual(sol, old_loc, older_loc, dist)
+                rmax, rl2, imax = self._norms(res, dsol, mask_own, dist)
+                cuts += 1
+            cuts_total += cuts
+            it += 1
+            if not (ok and it < max_nonlin_it and rmax < 1.0e20 and rmax > tol_nonlin and imax > inc_nonlin):
+                break
+        success = not (((rmax > tol_nonlin) and (imax > inc_nonlin)) or rmax >= 1.0e20 or not ok)
+        if not success:                                                              # fe_newton.c:893-899
+            sol = sol_old_own.copy()
+            sol[mask_own == 1] = dirichlet_own[mask_own == 1]
+        return sol, {"newton_its": it, "krylov_its": kry, "resid_max": rmax, "ok": success,
+                     "linesearch_cuts": cuts_total}

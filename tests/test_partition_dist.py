@@ -218,3 +218,59 @@ def test_distributed_residual_over_gloo():
     assert all(p.exitcode == 0 for p in procs)
     case, z = load("dump_wetdry_12.npz")
     assert np.array_equal(np.concatenate([out[r] for r in range(world)]), z["ref_residual"])
+
+
+def _newton_worker(rank, world, port, nsteps, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    from adh_kraken_b200.partition import RankNewton
+    case = small_delaunay_case(n=12, seed=5, nsteps=nsteps)
+    o = OracleModel(case)
+    rn = RankNewton(case, o.indptr, o.cols, world, rank, OracleModel)
+    r0, r1 = rn.r0, rn.r1
+    sol = case.sol0[r0:r1].copy(); old = sol.copy()
+    mask = np.zeros(r1 - r0, np.int32); dirichlet = np.zeros(r1 - r0)
+    hist, t = [], case.t0
+    for _ in range(nsteps):
+        t += case.dt
+        older, old = old, sol
+        rn.model.set_bc_window(t - case.dt, t)
+        sol, st = rn.solve(old, older, mask, dirichlet, dist, krylov_max_it=20000)
+        hist.append((st["newton_its"], st["linesearch_cuts"], st["ok"]))
+    out[rank] = (sol, hist)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_distributed_newton_steps_follow_the_single_process_run():
+    """Two ranks run the reference's Newton loop on their halo sub-meshes (norms, dots
+    and ghost columns through gloo): the same Newton iterations and line-search cuts as
+    the single-process oracle, the same states to 1e-10, and the reference's run to 1e-8."""
+    from fixtures import load
+    world, nsteps = 2, 4
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_newton_worker, args=(r, world, port, nsteps, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs)
+    case = small_delaunay_case(n=12, seed=5, nsteps=nsteps)
+    sol1, hist1 = OracleModel(case).run(nsteps, krylov_max_it=20000)
+    sold = np.concatenate([out[r][0] for r in range(world)])
+    assert out[0][1] == out[1][1]
+    assert [h[:2] for h in out[0][1]] == [(h["newton_its"], h["linesearch_cuts"]) for h in hist1]
+    assert all(h[2] for h in out[0][1])
+    for k in range(3):
+        a, b = sold[k::3], sol1[k::3]
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(b).max(), 1e-300), k
+    _, z = load("run_wetdry_12_4steps.npz")
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)[-1]
+    for k in range(3):
+        assert np.abs(sold[k::3] - ref[k::3]).max() <= 1e-8 * np.abs(ref[k::3]).max(), k
