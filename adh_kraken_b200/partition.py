@@ -334,7 +334,8 @@ class RankNewton:
     """fe_newton (src/newton/fe_newton.c:44-915) for one rank of a partitioned run:
     residual and Jacobian rows from the rank's halo sub-mesh (``make_model`` builds
     the element evaluator for it: an object with wd_flags / residual / jacobian on
-    local states, such as the CPU oracle or a device model), check_diag, Dirichlet
+    local states and the sub-mesh CSR row pointers, ``indptr`` or ``sparsity()`` --
+    the CPU oracle, or the device model, which offers the same calls), check_diag, Dirichlet
     rows and columns, row and column scaling, block-Jacobi BiCGStab over the split
     CSR, the line search and the stop tests, with the norms and dot products reduced
     over the ranks.  Column operations read the ghost columns' Dirichlet marks and
@@ -350,6 +351,7 @@ class RankNewton:
         self.send, self.recv = self.send[rank], self.recv[rank]
         sub, _ = part_case(case, self.part)
         self.model = make_model(sub)
+        self.sub_indptr = self.model.indptr if hasattr(self.model, "indptr") else self.model.sparsity()[0]
         self.plan = split(indptr, cols, np.zeros(len(cols)), case.nnodes, npes)[rank]
         self.r0, self.r1 = 3 * self.part.lo, 3 * self.part.hi
         rows = slice(int(indptr[self.r0]), int(indptr[self.r1]))
@@ -381,12 +383,12 @@ class RankNewton:
 
     def _jacobian(self, sol_own, old_loc, older_loc, dist):
         v = self.model.jacobian(self._local(sol_own, dist), old_loc, older_loc)
-        ip = self.model.indptr
+        ip = self.sub_indptr
         return np.concatenate([v[ip[r]:ip[r + 1]] for r in self.own_rows])
 
     def _norms(self, res, dsol, mask, dist):
         inc = mask != 1
-        rmax = _gmax(res[inc], dist) if True else 0.0
+        rmax = _gmax(res[inc], dist)
         l2 = _gsum(float(np.sum(res[inc] * res[inc])), dist)
         imax = _gmax(dsol[inc], dist)
         return rmax, np.sqrt(l2) / self.n_global, imax
