@@ -49,7 +49,8 @@ def parse():
     p.add_argument("--nx", type=int, default=2828)
     p.add_argument("--ny", type=int, default=707)
     p.add_argument("--krylov-tol", type=float, default=1e-6,
-                   help="inexact-Newton forcing: linear residual <= tol * Newton residual (floor tol_nonlin / 2)")
+                   help="inexact-Newton forcing: linear residual <= tol * Newton residual (floor: a tenth of "
+                        "tol_nonlin with the relative Newton test, a hundredth with the absolute one)")
     p.add_argument("--guess", choices=["none", "learned"], default="learned")
     p.add_argument("--weights", default=None, help="trained initial-guess weights (default: the committed ones)")
     p.add_argument("--tol-rel", type=float, default=1e-8,
