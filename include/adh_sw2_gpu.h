@@ -49,8 +49,10 @@ typedef struct {
     double inc_nonlin;        /* sm->inc_nonlin, default 1e-6 */
     int max_nonlin_it;        /* sm->max_nonlin_it, default 10 */
     int max_linesearch_cuts;  /* sm->max_nonlin_linesearch_cuts, default 5 */
-    int krylov_max_it;        /* BiCGStab iteration cap per solve */
-    double krylov_tol;        /* BiCGStab stopping tolerance (bcgstab_solver.c:20-21: 1e-11) */
+    int krylov_max_it;        /* Krylov iteration cap per Newton correction */
+    double krylov_tol;        /* BiCGStab: stopping tolerance (bcgstab_solver.c:20-21: 1e-11); GMRES: forcing
+                                 term, max|r| <= max(krylov_tol * max|R|, tol_nonlin / 10 (relative Newton test)
+                                 or / 100 (absolute)) on the unscaled linear residual */
     int krylov_precision;     /* 64: FP64 BiCGStab; 32: FP32 BiCGStab inside FP64 iterative refinement */
     double refine_tol;        /* FP32 inner solve relative reduction per refinement pass (32-bit mode) */
     int max_refine;           /* refinement passes per Newton correction (32-bit mode) */
@@ -58,9 +60,10 @@ typedef struct {
                                  L2 norm is below that of sol_old (else sol_old, the reference's start) */
     int precond;              /* SW2G_PC_AMG (default), SW2G_PC_BILU0 or SW2G_PC_BLOCK_JACOBI */
     int krylov_method;        /* SW2G_KRYLOV_GMRES (default; needs SW2G_PC_AMG or SW2G_PC_BILU0) or SW2G_KRYLOV_BICGSTAB */
-    double tol_nonlin_rel;    /* > 0: Newton residual test relative to the step's initial residual max-norm,
-                                 max|R| <= tol_nonlin_rel * max|R0| (replaces tol_nonlin); 0 (default): the
-                                 reference's absolute test */
+    double tol_nonlin_rel;    /* > 0: Newton residual test relative to the residual max-norm at the previous
+                                 step's state (the reference's starting point, the same whatever the initial
+                                 guess): max|R| <= tol_nonlin_rel * max|R(sol_old)| (replaces tol_nonlin);
+                                 0 (default): the reference's absolute test */
     int krylov_basis_precision; /* GMRES with krylov_precision 32: 64 (default) keeps the Krylov basis, the SpMV
                                  and the Gram-Schmidt in FP64 around the FP32 preconditioner; 32 runs the whole
                                  cycle in FP32, each cycle refined from the FP64 residual */
@@ -81,11 +84,11 @@ typedef struct {
 
 typedef struct {
     int newton_its;           /* Newton iterations of the step */
-    int krylov_its;           /* BiCGStab iterations summed over the step */
+    int krylov_its;           /* Krylov (BiCGStab or GMRES) iterations summed over the step */
     int linesearch_cuts;      /* line-search halvings summed over the step */
     int refine_passes;        /* FP64 refinement passes (32-bit mode) */
     int success;              /* fe_newton's TRUE/FALSE */
-    int krylov_breakdowns;    /* BiCGStab solves that stopped on a zero/non-finite denominator */
+    int krylov_breakdowns;    /* Krylov solves that stopped on a zero/non-finite denominator */
     double resid_max;         /* final max |R| over non-Dirichlet dofs */
     double resid_l2;          /* final sqrt(sum R^2)/ndofs */
     double inc_max;           /* last max |increment| */
