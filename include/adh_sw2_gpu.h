@@ -71,7 +71,7 @@ typedef struct {
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's
- * (bcgstab_solver.c:65-330).  GMRES(30), right-preconditioned and restarted from
+ * (bcgstab_solver.c:65-330).  GMRES(m) (m = krylov_restart), right-preconditioned and restarted from
  * the true FP64 residual, is robust where an approximate preconditioner leaves a
  * far-from-normal operator (BiCGStab's residual then swings or diverges). */
 #define SW2G_KRYLOV_BICGSTAB 0
