@@ -161,3 +161,18 @@ class SW2Simulation:
 
     def state(self):
         return self.model.store_state()
+
+    def checkpoint(self, path: str) -> None:
+        """Write the resident state -- the three solution levels, the Dirichlet marks,
+        the time and the step count -- to ``path`` (.npz).  Resuming from it with
+        :meth:`restore` takes the same next step as the uninterrupted run."""
+        sol, sol_old, sol_older, bc_mask = self.model.store_state()
+        np.savez(path, sol=sol, sol_old=sol_old, sol_older=sol_older, bc_mask=bc_mask, t=self.t,
+                 dt=self.case.dt, steps=len(self.history))
+
+    def restore(self, path: str) -> None:
+        z = np.load(path)
+        if float(z["dt"]) != self.case.dt or z["sol"].size != 3 * self.case.nnodes:
+            raise ValueError("checkpoint does not belong to this case")
+        self.model.load_state(z["sol"], z["sol_old"], z["sol_older"], bc_mask=z["bc_mask"])
+        self.t = float(z["t"])
