@@ -31,9 +31,13 @@ class OracleStepper:
         return self.sol.copy(), self.old.copy(), self.older.copy(), self.mask.copy()
 
     def step(self, opts=None):
+        self.before = (self.sol.copy(), self.old.copy(), self.older.copy())
         self.older, self.old = self.old, self.sol.copy()      # smodel_super_prep_sol
         st = self.o.newton(self.sol, self.old, self.older, self.mask, self.dirichlet, krylov_max_it=20000)
         return {"success": int(st["ok"]), "newton_its": st["newton_its"], "krylov_its": st["krylov_its"]}
+
+    def undo_step(self):
+        self.sol, self.old, self.older = self.before
 
     def grid_mass(self, sol=None, density=1.0, dt=None):
         s = self.sol if sol is None else sol
@@ -90,3 +94,34 @@ def test_mass_balance_and_retry_on_the_oracle_stepper():
     mb = sim.mass_balance()
     assert mb["steps"] == 3 and mb["inflow"] == inflow
     assert mb["error"] == abs(sim.model.o.grid_mass(sim.state()[0]) - inflow - m0)
+
+
+def test_failed_step_is_retried_with_a_quarter_dt():
+    """dt = 150 s fails on the wet/dry case (in the reference too); advance() undoes
+    it and covers the interval in four steps of 37.5 s, which converge and equal four
+    plain 37.5 s steps from the same start."""
+    import dataclasses
+    from adh_kraken_b200.timeloop import DT_REDUCE_FACTOR
+    case = small_delaunay_case(n=12, seed=5, nsteps=3, dt=150.0)
+    sim = SW2Simulation(case, model=OracleStepper(case))
+    st = sim.advance()
+    assert st["success"] == 1 and st["dt_cuts"] == 1 and st["substeps"] == 4
+    assert sim.t == case.t0 + case.dt and not sim.history[0]["success"]
+    small = dataclasses.replace(case, dt=case.dt * DT_REDUCE_FACTOR)
+    ref = SW2Simulation(small, model=OracleStepper(small))
+    ref.run(4)
+    assert np.array_equal(sim.state()[0], ref.state()[0])
+
+
+def test_nan_state_fails_every_retry():
+    """A NaN planted in the state (host side): every attempt fails, advance() gives up
+    after its reductions and leaves the state and the clock at the step's start."""
+    case = small_delaunay_case(n=12, seed=5, nsteps=3)
+    sim = SW2Simulation(case, model=OracleStepper(case))
+    sol = case.sol0.copy()
+    sol[3 * 7] = np.nan
+    sim.model.load_state(sol, sol, sol)
+    st = sim.advance(max_cuts=2)
+    assert st["success"] == 0 and st["dt_cuts"] == 3 and st["substeps"] == 0
+    assert sim.t == case.t0
+    assert np.isnan(sim.state()[0][3 * 7])
