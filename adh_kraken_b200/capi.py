@@ -254,6 +254,7 @@ class SW2Model:
 
     def set_profiling(self, on=True):
         self._check(lib().sw2g_set_profiling(self.h, int(on)))
+        self.profiling = bool(on)
 
     def profile(self):
         ms = np.zeros(6); n = np.zeros(6, np.int64)

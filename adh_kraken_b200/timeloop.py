@@ -73,6 +73,7 @@ class SW2Simulation:
         self.model.load_state(sol0, sol0, sol0)
         self.history = []
         self.mass_log = None
+        self.log = None     # a writable text stream: one JSON line per step (set_log)
 
     def bc_values(self, t1, t2):
         s = self.case.series
@@ -97,11 +98,37 @@ class SW2Simulation:
         st = self.model.step(opts or self.opts)
         self.t = t_new
         self.history.append(st)
+        rec = None
         if self.mass_log is not None and st["success"]:
             m, inflow = self.model.grid_mass(None, self.density, dt)
             self.inflow_total += inflow
             self.mass_log.append((t_new, m, inflow))
+            rec = (m, inflow)
+        if self.log is not None:
+            self._write_log(t_new, dt, st, rec)
         return st
+
+    def set_log(self, stream) -> None:
+        """Write one JSON line per step to ``stream`` (None stops): time, dt, the Newton
+        statistics, the grid mass and boundary inflow when the mass balance is on, and
+        the device time per kernel class accumulated since the last profile reset when
+        the model profiles (set_profiling)."""
+        self.log = stream
+
+    def _write_log(self, t, dt, st, mass):
+        import json
+        keys = ("success", "newton_its", "krylov_its", "linesearch_cuts", "resid_max", "initial_resid_max",
+                "guess_used", "guess_fallback")
+        out = {"t": t, "dt": dt}
+        out.update({k: (float(st[k]) if isinstance(st[k], (float, np.floating)) else int(st[k]))
+                    for k in keys if k in st})
+        if mass is not None:
+            out["mass"], out["inflow"] = float(mass[0]), float(mass[1])
+        prof = getattr(self.model, "profile", None)
+        if getattr(self.model, "profiling", False) and prof is not None:
+            ms, n = prof()
+            out["class_ms_total"] = [round(float(x), 3) for x in ms]
+        self.log.write(json.dumps(out) + "\n")
 
     def advance(self, opts=None, max_cuts=3):
         """One step of the case's dt that survives failed Newton solves.  A failed

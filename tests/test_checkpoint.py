@@ -125,3 +125,19 @@ def test_nan_state_fails_every_retry():
     assert st["success"] == 0 and st["dt_cuts"] == 3 and st["substeps"] == 0
     assert sim.t == case.t0
     assert np.isnan(sim.state()[0][3 * 7])
+
+
+def test_per_step_json_log():
+    import io
+    import json
+    case = small_delaunay_case(n=12, seed=5, nsteps=3)
+    sim = SW2Simulation(case, model=OracleStepper(case))
+    buf = io.StringIO()
+    sim.set_log(buf)
+    sim.start_mass_balance(1000.0)
+    sim.run(3)
+    lines = [json.loads(x) for x in buf.getvalue().splitlines()]
+    assert len(lines) == 3
+    assert [ln["newton_its"] for ln in lines] == [h["newton_its"] for h in sim.history]
+    assert lines[-1]["t"] == sim.t and lines[0]["dt"] == case.dt and all(ln["success"] == 1 for ln in lines)
+    assert [ln["mass"] for ln in lines] == [m for _, m, _ in sim.mass_log]
