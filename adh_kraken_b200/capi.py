@@ -25,6 +25,7 @@ EXPORTED = [
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
     "sw2g_assemble_residual_noalloc", "sw2g_grid_mass", "sw2g_undo_step",
+    "sw2g_assemble_residual_wd", "sw2g_assemble_jacobian_wd",
     # include/adh_sw2_gnn.h (learned initial guess)
     "sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
     "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj",
@@ -81,8 +82,16 @@ def lib():
     return _LIB
 
 
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_MESH, ERR_NONFINITE = -1, -2, -3, -4, -5   # SW2G_ERR_* of adh_sw2_gpu.h
+
+
 class SW2Error(RuntimeError):
-    pass
+    """A non-zero status from the C ABI; ``rc`` holds the SW2G_ERR_* code (None when raised
+    by host code)."""
+
+    def __init__(self, msg, rc=None):
+        super().__init__(msg)
+        self.rc = rc
 
 
 def _d(a):
@@ -128,7 +137,7 @@ class SW2Model:
     # ------------------------------------------------------------- plumbing
     def _check(self, rc):
         if rc != 0:
-            raise SW2Error(f"sw2g error {rc}: {lib().sw2g_last_error().decode()}")
+            raise SW2Error(f"sw2g error {rc}: {lib().sw2g_last_error().decode()}", rc)
 
     def close(self):
         if getattr(self, "h", None):
@@ -179,6 +188,22 @@ class SW2Model:
     def jacobian(self, sol, sol_old, sol_older):
         v = np.zeros(self.nnz)
         self._check(lib().sw2g_assemble_jacobian(self.h, _d(_f64(sol)), _d(_f64(sol_old)), _d(_f64(sol_older)), _d(v)))
+        return v
+
+    def residual_wd(self, sol, sol_old, sol_older, wd_flag):
+        """The residual with the caller's wet/dry flags (sw2g_assemble_residual_wd)."""
+        r = np.zeros(self.ndofs)
+        wd = np.ascontiguousarray(wd_flag, dtype=np.int32)
+        self._check(lib().sw2g_assemble_residual_wd(self.h, _d(_f64(sol)), _d(_f64(sol_old)), _d(_f64(sol_older)),
+                                                    _i(wd), _d(r)))
+        return r
+
+    def jacobian_wd(self, sol, sol_old, sol_older, wd_flag):
+        """The CSR values with the caller's wet/dry flags (sw2g_assemble_jacobian_wd)."""
+        v = np.zeros(self.nnz)
+        wd = np.ascontiguousarray(wd_flag, dtype=np.int32)
+        self._check(lib().sw2g_assemble_jacobian_wd(self.h, _d(_f64(sol)), _d(_f64(sol_old)), _d(_f64(sol_older)),
+                                                    _i(wd), _d(v)))
         return v
 
     def prepare_system(self, vals, residual, x, bc_mask):

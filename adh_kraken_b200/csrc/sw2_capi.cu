@@ -47,6 +47,7 @@ struct ProfRec { int cls; cudaEvent_t a, b; };
 
 struct sw2g_model {
     int V = 0, T = 0, S = 0, Etot = 0, n = 0, nnz = 0, nslots = 0;
+    int device = 0;   // the device current at sw2g_create: every buffer and the stream live there
     cudaStream_t st = nullptr; bool own_stream = false;
     std::vector<int> h_indptr, h_cols;
     std::vector<void*> allocs;
@@ -197,6 +198,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
     for (long i = 0; i < 2L * S; i++) if (mesh->seg[i] < 0 || mesh->seg[i] >= V) { g_err = "sw2g_create: segment node id out of range"; return SW2G_ERR_MESH; }
     sw2g_model* m = new sw2g_model();
     m->V = V; m->T = T; m->S = S; m->Etot = T + S; m->n = 3 * V;
+    if (cudaGetDevice(&m->device) != cudaSuccess) { g_err = "sw2g_create: no current CUDA device"; delete m; return SW2G_ERR_CUDA; }
     if (cuda_stream) m->st = (cudaStream_t)cuda_stream;
     else {
         cudaError_t e = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking);
@@ -864,6 +866,8 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
     double prev = 0;
     int stall = 0;
     int hstate[4] = {0, 0, 0, 0};
+    double hscal[3] = {0, 0, 0};
+    static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;   // diagnostic: pass history on stderr
     for (int pass = 0;; pass++) {
         {
             ProfScope ps(m, 4, 2);
@@ -873,12 +877,17 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         }
         CK(cudaMemcpyAsync(m->h_rout, m->d_rout, sizeof(double), cudaMemcpyDeviceToHost, m->st));
         if (pass > 0) CK(cudaMemcpyAsync(hstate, m->gm.state, sizeof(int) * 3, cudaMemcpyDeviceToHost, m->st));
+        if (pass > 0 && trace) CK(cudaMemcpyAsync(hscal, m->gm.scal, sizeof(double) * 3, cudaMemcpyDeviceToHost, m->st));
         CK(cudaStreamSynchronize(m->st));
         if (pass > 0) {
             *iters += hstate[1];
             if (hstate[2] == 2) { *status = 2; break; }
         }
         const double rn = m->h_rout[0];
+        if (trace)
+            fprintf(stderr, "gmres pass %d max|r| %.3e target %.3e inner %d status %d cycle-reduction %.3e\n", pass, rn,
+                    target, pass > 0 ? hstate[1] : 0, pass > 0 ? hstate[2] : 0,
+                    (pass > 0 && hscal[0] > 0) ? hscal[2] / hscal[0] : 0.0);
         if (!std::isfinite(rn)) { *status = 2; break; }
         if (!(rn > target)) break;
         if (pass > 0) {
@@ -1242,6 +1251,39 @@ extern "C" int sw2g_assemble_jacobian(sw2g_model* m, const double* sol, const do
     return SW2G_OK;
 }
 
+// The same two assemblies with the caller's wet/dry flags: inside fe_newton the
+// reference evaluates every residual and Jacobian of a Newton solve with the flags
+// fe_sw2_init set at its start (initialize_system, newton_tools.c:21-53), not with
+// flags of the current iterate.
+static int put_wd(sw2g_model* m, const int* wd_flag) {
+    for (int e = 0; e < m->T; e++)
+        if (wd_flag[e] < 0 || wd_flag[e] > 2) { g_err = "wet/dry flags must be 0, 1 or 2"; return SW2G_ERR_ARG; }
+    CK(cudaMemcpyAsync(m->d_wd, wd_flag, sizeof(int) * m->T, cudaMemcpyHostToDevice, m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_assemble_residual_wd(sw2g_model* m, const double* sol, const double* sol_old,
+                                         const double* sol_older, const int* wd_flag, double* residual) {
+    NEED(m && sol && sol_old && sol_older && wd_flag && residual, "sw2g_assemble_residual_wd: null argument");
+    TRY(put_wd(m, wd_flag));
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_residual(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_res));
+    CK(cudaMemcpyAsync(residual, m->d_res, sizeof(double) * m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
+extern "C" int sw2g_assemble_jacobian_wd(sw2g_model* m, const double* sol, const double* sol_old,
+                                         const double* sol_older, const int* wd_flag, double* vals) {
+    NEED(m && sol && sol_old && sol_older && wd_flag && vals, "sw2g_assemble_jacobian_wd: null argument");
+    TRY(put_wd(m, wd_flag));
+    TRY(put3(m, sol, sol_old, sol_older));
+    TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
+    CK(cudaMemcpyAsync(vals, m->d_vals, sizeof(double) * m->nnz, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return SW2G_OK;
+}
+
 extern "C" int sw2g_prepare_system(sw2g_model* m, double* vals, double* residual, double* x, int* bc_mask, double* scale) {
     NEED(m && vals && residual && x && bc_mask && scale, "sw2g_prepare_system: null argument");
     const size_t n = m->n;
@@ -1481,9 +1523,15 @@ static NoAllocScratch g_na_ptr[kNoAllocMaxDevices];
 static bool g_na_ready[kNoAllocMaxDevices];
 static std::mutex g_na_mutex;
 
-static int noalloc_scratch(NoAllocScratch* out) {
+static int noalloc_scratch(const sw2g_model* m, NoAllocScratch* out) {
+    // cudaGetSymbolAddress answers for the current device, so that must be the model's
     int dev = 0;
     CK(cudaGetDevice(&dev));
+    if (dev != m->device) {
+        g_err = "sw2g_assemble_residual_noalloc: the current device is not the model's (make the device that was "
+                "current at sw2g_create current again)";
+        return SW2G_ERR_ARG;
+    }
     if (dev < 0 || dev >= kNoAllocMaxDevices) { g_err = "sw2g_assemble_residual_noalloc: device index too large"; return SW2G_ERR_ARG; }
     std::lock_guard<std::mutex> lock(g_na_mutex);
     if (!g_na_ready[dev]) {
@@ -1507,7 +1555,7 @@ extern "C" int sw2g_assemble_residual_noalloc(sw2g_model* m, const double* d_sol
         return SW2G_ERR_ARG;
     }
     NoAllocScratch S{};
-    TRY(noalloc_scratch(&S));
+    TRY(noalloc_scratch(m, &S));
     // every entry of the three arrays that the gather reads is written first by this call
     // (wet/dry node marks, element flags, 9 (6) residual entries per triangle (segment)), so
     // nothing needs clearing between calls

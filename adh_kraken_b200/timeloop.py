@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .capi import SW2Error, SW2Model, default_opts
+from .capi import ERR_NONFINITE, SW2Error, SW2Model, default_opts
 
 _EPS = np.finfo(np.float64).eps
 DT_REDUCE_FACTOR = 0.25        # tc_scale's factor after a failed Newton solve (src/include/define.h:127)
@@ -71,7 +71,8 @@ class SW2Simulation:
         self.t = case.t0
         sol0 = case.sol0.astype(np.float64)
         self.model.load_state(sol0, sol0, sol0)
-        self.history = []
+        self.history = []        # every Newton solve tried, failed ones included
+        self.nsteps_done = 0     # successful steps (what a checkpoint counts)
         self.mass_log = None
         self.log = None     # a writable text stream: one JSON line per step (set_log)
 
@@ -90,29 +91,49 @@ class SW2Simulation:
         self.model.set_step(dt, d, vx, vy)
         return t_new
 
-    def step(self, opts=None, dt=None):
-        """One Newton solve over [t, t + dt] (dt: the case's step by default).  A failed
-        solve leaves the state at the step's start, as fe_newton does, and time moves on."""
-        dt = self.case.dt if dt is None else dt
+    def _attempt(self, opts, dt):
+        """One Newton solve over [t, t + dt]; the clock stays.  A non-finite residual
+        (SW2G_ERR_NONFINITE) is a failed solve like any other; every other error --
+        bad arguments, CUDA errors, errors of set_step -- propagates."""
         t_new = self.prepare_step(dt)
-        st = self.model.step(opts or self.opts)
-        self.t = t_new
+        try:
+            st = self.model.step(opts or self.opts)
+        except SW2Error as e:
+            if e.rc != ERR_NONFINITE:
+                raise
+            st = {"success": 0, "newton_its": 0, "krylov_its": 0, "error": str(e)}
+        return st, t_new
+
+    def _record(self, st, t_new, dt, moved):
         self.history.append(st)
         rec = None
-        if self.mass_log is not None and st["success"]:
-            m, inflow = self.model.grid_mass(None, self.density, dt)
-            self.inflow_total += inflow
-            self.mass_log.append((t_new, m, inflow))
-            rec = (m, inflow)
+        if moved:
+            self.t = t_new
+        if st["success"]:
+            self.nsteps_done += 1
+            if self.mass_log is not None:
+                m, inflow = self.model.grid_mass(None, self.density, dt)
+                self.inflow_total += inflow
+                self.mass_log.append((t_new, m, inflow))
+                rec = (m, inflow)
         if self.log is not None:
             self._write_log(t_new, dt, st, rec)
+
+    def step(self, opts=None, dt=None):
+        """One Newton solve over [t, t + dt] (dt: the case's step by default) with the
+        reference's semantics: a failed solve leaves the state at the step's start, as
+        fe_newton does, and time moves on (the reference's time loop then stops,
+        src/timeloop/time_loop.c:37).  advance() is the form that retries instead."""
+        dt = self.case.dt if dt is None else dt
+        st, t_new = self._attempt(opts, dt)
+        self._record(st, t_new, dt, moved=True)
         return st
 
     def set_log(self, stream) -> None:
-        """Write one JSON line per step to ``stream`` (None stops): time, dt, the Newton
-        statistics, the grid mass and boundary inflow when the mass balance is on, and
-        the device time per kernel class accumulated since the last profile reset when
-        the model profiles (set_profiling)."""
+        """Write one JSON line per Newton solve to ``stream`` (None stops): time, dt, the
+        Newton statistics, the grid mass and boundary inflow when the mass balance is on,
+        and the device time per kernel class accumulated since the last profile reset
+        when the model profiles (set_profiling)."""
         self.log = stream
 
     def _write_log(self, t, dt, st, mass):
@@ -130,40 +151,53 @@ class SW2Simulation:
             out["class_ms_total"] = [round(float(x), 3) for x in ms]
         self.log.write(json.dumps(out) + "\n")
 
-    def advance(self, opts=None, max_cuts=3):
-        """One step of the case's dt that survives failed Newton solves.  A failed
+    def advance(self, opts=None, max_cuts=3, before_attempt=None):
+        """One interval of the case's dt that survives failed Newton solves.  A failed
         solve is undone and the interval is tried again with dt scaled by
         DT_REDUCE_FACTOR, as tc_scale scales it (src/tools/tc_scale.c:10, called at
         src/newton/fe_newton.c:887); the rest of the interval is then covered in
         steps of the reduced size.  The reference instead ends its time loop at the
         first failure (src/timeloop/time_loop.c:37).  Gives up after max_cuts
-        reductions (success 0, the state at the last good substep)."""
+        reductions (success 0, the state and the clock at the last good substep).
+        ``before_attempt(sim)``, when given, runs before every Newton solve (e.g. to
+        set an initial guess).  Failed attempts are undone before anything else runs:
+        the clock never moves for them and the mass log never sees them."""
         target = self.t + self.case.dt
-        dt, cuts, subs = self.case.dt, 0, []
+        dt, cuts, subs, failed = self.case.dt, 0, [], []
         while self.t + NOT_QUITE_SMALL * self.case.dt < target:
             h = min(dt, target - self.t)
-            t_start = self.t
-            try:
-                st = self.step(opts, dt=h)
-            except SW2Error:               # a non-finite residual: a failed solve like any other
-                st = {"success": 0}
+            if before_attempt is not None:
+                before_attempt(self)
+            st, t_new = self._attempt(opts, h)
             if st["success"]:
+                self._record(st, t_new, h, moved=True)
                 subs.append(st)
                 continue
             self.model.undo_step()
-            self.t = t_start
+            self._record(st, t_new, h, moved=False)
+            failed.append(st)
             cuts += 1
             if cuts > max_cuts:
                 break
             dt = h * DT_REDUCE_FACTOR
         ok = cuts <= max_cuts
-        return {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts,
-                "newton_its": sum(s["newton_its"] for s in subs), "krylov_its": sum(s["krylov_its"] for s in subs)}
+        out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts,
+               "newton_its": sum(s["newton_its"] for s in subs + failed),
+               "krylov_its": sum(s["krylov_its"] for s in subs + failed)}
+        if subs:
+            last = subs[-1]
+            for k in ("resid_max", "inc_max", "tol_used"):
+                if k in last:
+                    out[k] = last[k]
+            for k in ("prev_resid_max", "initial_resid_max", "guess_used"):
+                if k in subs[0]:
+                    out[k] = subs[0][k]
+        return out
 
     def start_mass_balance(self, density=1.0):
         """Start the mass bookkeeping of tl_find_grid_mass_error_elem2d
-        (src/tools/tl_grid_mass.c:280) from the resident state: every later step
-        records the grid mass of its result and its boundary mass inflow."""
+        (src/tools/tl_grid_mass.c:280) from the resident state: every later successful
+        step records the grid mass of its result and its boundary mass inflow."""
         self.density = float(density)
         self.mass0, _ = self.model.grid_mass(None, self.density, self.case.dt)
         self.inflow_total = 0.0
@@ -191,11 +225,17 @@ class SW2Simulation:
 
     def checkpoint(self, path: str) -> None:
         """Write the resident state -- the three solution levels, the Dirichlet marks,
-        the time and the step count -- to ``path`` (.npz).  Resuming from it with
-        :meth:`restore` takes the same next step as the uninterrupted run."""
+        the time, the count of successful steps and, when the mass balance is on, its
+        totals and log -- to ``path`` (.npz).  Resuming from it with :meth:`restore`
+        takes the same next step, and reports the same mass error, as the
+        uninterrupted run."""
         sol, sol_old, sol_older, bc_mask = self.model.store_state()
+        extra = {}
+        if self.mass_log is not None:
+            extra = {"mass_density": self.density, "mass0": self.mass0, "mass_inflow_total": self.inflow_total,
+                     "mass_log": np.asarray(self.mass_log, dtype=np.float64).reshape(-1, 3)}
         np.savez(path, sol=sol, sol_old=sol_old, sol_older=sol_older, bc_mask=bc_mask, t=self.t,
-                 dt=self.case.dt, steps=len(self.history))
+                 dt=self.case.dt, steps=self.nsteps_done, **extra)
 
     def restore(self, path: str) -> None:
         z = np.load(path)
@@ -203,3 +243,11 @@ class SW2Simulation:
             raise ValueError("checkpoint does not belong to this case")
         self.model.load_state(z["sol"], z["sol_old"], z["sol_older"], bc_mask=z["bc_mask"])
         self.t = float(z["t"])
+        self.nsteps_done = int(z["steps"])
+        if "mass0" in z:
+            self.density = float(z["mass_density"])
+            self.mass0 = float(z["mass0"])
+            self.inflow_total = float(z["mass_inflow_total"])
+            self.mass_log = [tuple(float(v) for v in row) for row in z["mass_log"]]
+        else:
+            self.mass_log = None

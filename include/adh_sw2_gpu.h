@@ -137,6 +137,14 @@ int sw2g_assemble_residual(sw2g_model *m, const double *sol, const double *sol_o
 /* assemble_jacobian(SMODEL_SUPER*) (src/jacobian/jacobian.h:5): CSR values [nnz] */
 int sw2g_assemble_jacobian(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
                            double *vals);
+/* The same assemblies with the caller's wet/dry flags [ntri] (0, 1 or 2): what
+ * assemble_residual / assemble_jacobian compute inside fe_newton, whose element
+ * routines read sm->dvars.elem_flags[_WDFLAG] as fe_sw2_init set it at the start of
+ * the Newton solve (src/newton/newton_tools.c:21-53, src/models/sw2/sw2_body_resid.c:88). */
+int sw2g_assemble_residual_wd(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                              const int *wd_flag, double *residual);
+int sw2g_assemble_jacobian_wd(sw2g_model *m, const double *sol, const double *sol_old, const double *sol_older,
+                              const int *wd_flag, double *vals);
 /* check_diag + apply_Dirichlet_BC (src/la/la.h:12-13) + scale_linear_system (la.h:46):
  * vals [nnz], residual [ndofs], x [ndofs] and bc_mask [ndofs] in/out; scale [ndofs] out. */
 int sw2g_prepare_system(sw2g_model *m, double *vals, double *residual, double *x, int *bc_mask, double *scale);
@@ -173,9 +181,10 @@ int sw2g_grid_mass(sw2g_model *m, const double *sol, double density, double dt, 
  * GPU that loads it until the process exits), so the mesh may have at most 131072
  * elements (triangles + segments) and 131072 nodes; larger meshes get SW2G_ERR_ARG.
  * d_sol, d_sol_old, d_sol_older [ndofs] and d_residual [ndofs] are device pointers on
- * the model's device; the step parameters come from sw2g_set_step.  The first call on a
- * device looks the arrays' device addresses up (once per device); make it before any
- * stream capture.  Every call shares the arrays, so calls that overlap on the GPU
+ * the model's device; the step parameters come from sw2g_set_step.  The model's device
+ * (the one current at sw2g_create) must be the current device when this is called
+ * (SW2G_ERR_ARG otherwise).  The first call on a device looks the arrays' device
+ * addresses up (once per device); make it before any stream capture.  Every call shares the arrays, so calls that overlap on the GPU
  * (other models, streams or host threads) race; the call returns after its kernels
  * have finished on the model's stream. */
 int sw2g_assemble_residual_noalloc(sw2g_model *m, const double *d_sol, const double *d_sol_old,

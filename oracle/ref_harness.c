@@ -36,13 +36,22 @@
  *  (vi)  selem1d_init_alloc_array writes through node arrays it never allocated
  *        (selem_1d.c:86-125); see build_grid.
  *
- * Usage: adh_ref_harness <dump|run|time|mass> <case.bin> <out.bin> [every|reps]
+ * Built a second time with -DSW2_REFGLUE into adh_refglue_harness: the reference's
+ * objects without src/residual/assemble_residual.c and src/jacobian/assemble_jacobian.c,
+ * linked with adh_kraken_b200/refglue/sw2_refglue.c, whose assemble_residual /
+ * assemble_jacobian run on the GPU; mode "loop" then runs the reference's own Newton
+ * on GPU assemblies and mode "loop_gpu" installs fe_newton_gpu as the stepper.
+ *
+ * Usage: adh_ref_harness <dump|run|loop|time|mass> <case.bin> <out.bin> [every|reps]
  *        adh_ref_harness init <case.bin> <out.bin> <init file base>
  *        adh_ref_harness geo <grid.geo> <out.bin>
  *        adh_ref_harness rect - <out.bin> xmin xmax ymin ymax npx npy a0 ax
  */
 #include "adh.h"
 #include <stdint.h>
+#ifdef SW2_REFGLUE
+#include "sw2_refglue.h"
+#endif
 
 SADH_DEF adh_def; /* defined by src/main/adh.c in the reference binary */
 
@@ -242,8 +251,52 @@ static void build_model(const CASE *c) {
 }
 
 /* ---------------------------------------------------------------- modes */
+/* The reference's own time loop (src/timeloop/time_loop.c:14-89: tc_init, update_dt,
+ * advance_time -> adh_time_stepper[sm->forward_step]) over the case's steps.  The
+ * stepper installed in adh_time_stepper[FE_NEWTON] is wrapped so that every step's
+ * state, success flag and Newton count are recorded as the loop runs. */
+static int (*g_inner_stepper)(SMODEL_SUPER *) = NULL;
+static int g_loop_steps = 0, g_loop_cap = 0;
+static double *g_loop_sol = NULL;
+static int *g_loop_ok = NULL, *g_loop_its = NULL;
+static double *g_loop_secs = NULL;
+
+static double now_s(void);
+static int recording_stepper(SMODEL_SUPER *sm) {
+    const int before = sm->it_count_nonlin;
+    const double t0 = now_s();
+    const int r = g_inner_stepper(sm);
+    if (g_loop_steps < g_loop_cap) {
+        memcpy(g_loop_sol + (size_t)sm->ndofs * g_loop_steps, sm->sol, sizeof(double) * sm->ndofs);
+        g_loop_ok[g_loop_steps] = r;
+        g_loop_its[g_loop_steps] = sm->it_count_nonlin - before;
+        g_loop_secs[g_loop_steps] = now_s() - t0;
+    }
+    g_loop_steps++;
+    return r;
+}
+
+static void mode_loop(const CASE *c, int (*stepper)(SMODEL_SUPER *)) {
+    SMODEL_SUPER *sm = g_sm;
+    g_loop_cap = c->nsteps + 2;
+    g_loop_sol = calloc((size_t)sm->ndofs * g_loop_cap, sizeof(double));
+    g_loop_ok = calloc(g_loop_cap, sizeof(int));
+    g_loop_its = calloc(g_loop_cap, sizeof(int));
+    g_loop_secs = calloc(g_loop_cap, sizeof(double));
+    g_inner_stepper = stepper;
+    adh_time_stepper[FE_NEWTON] = recording_stepper;
+    time_loop(&g_dm);
+    const int n = g_loop_steps < g_loop_cap ? g_loop_steps : g_loop_cap;
+    out_rec("newton_its", 'i', g_loop_its, n);
+    out_rec("step_ok", 'i', g_loop_ok, n);
+    out_rec("step_seconds", 'd', g_loop_secs, n);
+    out_rec("sol_steps", 'd', g_loop_sol, (int64_t)sm->ndofs * n);
+    out_rec("bc_mask", 'i', sm->bc_mask, sm->ndofs);
+}
+
 static double now_s(void) { struct timespec ts; clock_gettime(CLOCK_MONOTONIC, &ts); return ts.tv_sec + 1e-9 * ts.tv_nsec; }
 
+#ifndef SW2_REFGLUE
 static void mode_dump(const CASE *c) {
     SMODEL_SUPER *sm = g_sm; SGRID *grid = sm->grid; SLIN_SYS *ls = sm->lin_sys;
     int V = grid->nnodes, T = grid->nelems2d, S = grid->nelems1d, N = sm->ndofs;
@@ -318,6 +371,8 @@ static void mode_dump(const CASE *c) {
         out_rec("dsol", 'd', ls->dsol, N);
     }
 }
+
+#endif
 
 static void mode_run(const CASE *c, int every) {
     SMODEL_SUPER *sm = g_sm; int N = sm->ndofs;
@@ -484,7 +539,14 @@ int main(int argc, char **argv) {
     build_model(&c);
     g_out = fopen(argv[3], "wb");
     if (!g_out) { fprintf(stderr, "harness: cannot write %s\n", argv[3]); return 2; }
+#ifndef SW2_REFGLUE
     if (strcmp(argv[1], "dump") == 0) mode_dump(&c);
+    else
+#endif
+    if (strcmp(argv[1], "loop") == 0) mode_loop(&c, fe_newton);
+#ifdef SW2_REFGLUE
+    else if (strcmp(argv[1], "loop_gpu") == 0) { mode_loop(&c, fe_newton_gpu); sw2_gpu_detach_all(); }
+#endif
     else if (strcmp(argv[1], "run") == 0) mode_run(&c, argc > 4 ? atoi(argv[4]) : 1);
     else if (strcmp(argv[1], "time") == 0) mode_time(&c, argc > 4 ? atoi(argv[4]) : 1);
     else if (strcmp(argv[1], "mass") == 0) mode_mass(&c);

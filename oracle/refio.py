@@ -17,10 +17,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "_ref", "adh_ref_harness")
+# the reference's objects with assemble_residual / assemble_jacobian taken from the
+# product's reference-signature glue (GPU); runs only where a GPU is present
+GLUE_HARNESS = os.path.join(HERE, "_ref", "adh_refglue_harness")
 
 
-def harness_available() -> bool:
-    return os.path.exists(HARNESS)
+def harness_available(binary=HARNESS) -> bool:
+    return os.path.exists(binary)
 
 
 def write_case(case, path, sol=None, sol_old=None, sol_older=None):
@@ -63,9 +66,9 @@ def read_records(path):
 
 
 def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=None, env=None, timeout=3600,
-                in_path=None):
-    if not harness_available():
-        raise RuntimeError("reference harness not built (oracle/_ref/adh_ref_harness)")
+                in_path=None, binary=HARNESS):
+    if not harness_available(binary):
+        raise RuntimeError(f"reference harness not built ({binary})")
     with tempfile.TemporaryDirectory() as td:
         cpath = os.path.join(td, "case.bin")
         opath = os.path.join(td, "out.bin")
@@ -79,7 +82,7 @@ def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=Non
         if env:
             e.update(env)
         # cwd: the reference's grid reader writes a node listing file into the working directory
-        r = subprocess.run([HARNESS, mode, cpath, opath, *map(str, extra)], capture_output=True, env=e,
+        r = subprocess.run([binary, mode, cpath, opath, *map(str, extra)], capture_output=True, env=e,
                            timeout=timeout, cwd=td)
         if r.returncode != 0:
             raise RuntimeError(f"harness {mode} failed ({r.returncode}): {r.stderr.decode()[-2000:]}")

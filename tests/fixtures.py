@@ -6,6 +6,18 @@ import numpy as np
 from adh_kraken_b200.mesh import SW2Case
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def reference_src():
+    """The reference tree's src/ directory as oracle/Makefile recorded it when it
+    compiled the reference (oracle/_ref/ref_src_path.txt), or None where that tree is
+    not on this machine (the tests that read it then skip)."""
+    rec = os.path.join(ROOT, "oracle", "_ref", "ref_src_path.txt")
+    if not os.path.exists(rec):
+        return None
+    path = open(rec).read().strip()
+    return path if os.path.exists(os.path.join(path, "include", "adh.h")) else None
 
 
 def load(name):

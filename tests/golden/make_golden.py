@@ -115,6 +115,8 @@ def main():
     run_fixture("run_flume_21x6_8steps.npz", flume_case(nsteps=8, npx=21, npy=6))
     run_fixture("run_wetdry_12_4steps.npz", small_delaunay_case(n=12, seed=5, nsteps=4))
     run_fixture("run_still_beach_16x6_1440steps.npz", still_beach_case(nsteps=1440), every=240)
+    # the CPU-runnable benchmark configuration: 101 x 11 flume, 100 steps of 60 s (every 10th state kept)
+    run_fixture("run_flume_101x11_100steps.npz", flume_case(nsteps=100), every=10)
     run_fixture("run_basin_12_6steps.npz", basin_case(n=12, seed=2, nsteps=6))
     # dt 600 s: four line-search halvings in the first Newton solve; dt 150 s: a failed solve
     run_fixture("run_wetdry_12_dt600_6steps.npz", small_delaunay_case(n=12, seed=5, nsteps=6, dt=600.0))

@@ -37,7 +37,11 @@ class OracleStepper:
         return {"success": int(st["ok"]), "newton_its": st["newton_its"], "krylov_its": st["krylov_its"]}
 
     def undo_step(self):
-        self.sol, self.old, self.older = self.before
+        # as sw2g_undo_step turns the level rotation back: the start state and its
+        # previous level return, the sol_older level keeps the failed step's buffer
+        failed = self.sol
+        self.sol, self.old = self.before[0], self.before[1]
+        self.older = failed
 
     def grid_mass(self, sol=None, density=1.0, dt=None):
         s = self.sol if sol is None else sol
@@ -141,3 +145,25 @@ def test_per_step_json_log():
     assert [ln["newton_its"] for ln in lines] == [h["newton_its"] for h in sim.history]
     assert lines[-1]["t"] == sim.t and lines[0]["dt"] == case.dt and all(ln["success"] == 1 for ln in lines)
     assert [ln["mass"] for ln in lines] == [m for _, m, _ in sim.mass_log]
+
+
+def test_resume_keeps_step_count_and_mass_balance(tmp_path):
+    """The checkpoint carries the count of successful steps and the mass bookkeeping
+    (initial mass, boundary inflow so far, the per-step log): a resumed run reports the
+    same mass error as the uninterrupted one."""
+    case = small_delaunay_case(n=12, seed=5, nsteps=4)
+    full = SW2Simulation(case, model=OracleStepper(case))
+    full.start_mass_balance(1000.0)
+    full.run(4)
+    first = SW2Simulation(case, model=OracleStepper(case))
+    first.start_mass_balance(1000.0)
+    first.run(2)
+    ck = str(tmp_path / "ck.npz")
+    first.checkpoint(ck)
+    resumed = SW2Simulation(case, model=OracleStepper(case))
+    resumed.restore(ck)
+    assert resumed.nsteps_done == 2
+    resumed.run(2)
+    assert resumed.nsteps_done == full.nsteps_done == 4
+    assert resumed.mass_balance() == full.mass_balance()
+    assert resumed.mass_log == full.mass_log

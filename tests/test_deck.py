@@ -12,7 +12,10 @@ from oracle.oracle import OracleModel
 from oracle.refio import harness_available, run_harness
 
 needs_harness = pytest.mark.skipif(not harness_available(), reason="reference harness not built")
-QA_GEO = "/root/reference/qa/flume/test.geo"
+from fixtures import reference_src
+
+_SRC = reference_src()
+QA_GEO = os.path.join(os.path.dirname(_SRC), "qa", "flume", "test.geo") if _SRC else None
 
 
 def cases():
@@ -55,7 +58,7 @@ def test_geo_reader_matches_reference(tmp_path, ci):
 
 
 @needs_harness
-@pytest.mark.skipif(not os.path.exists(QA_GEO), reason="reference QA deck not present")
+@pytest.mark.skipif(QA_GEO is None or not os.path.exists(QA_GEO), reason="reference QA deck not present")
 def test_geo_reader_on_the_reference_qa_grid():
     """The reference's own QA flume grid (comment lines, unordered cards, no materials
     on the element cards) read by both readers."""

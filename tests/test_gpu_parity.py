@@ -10,30 +10,37 @@ from oracle.oracle import OracleModel
 pytestmark = pytest.mark.gpu
 
 DUMPS = ["dump_flume_21x6.npz", "dump_wetdry_12.npz"]
+# the three-level scheme (tau_temporal 0.5) and a sixth of the nodes at depths 0, -0,
+# +-1e-20 and 1e-300: element and assembly parity only (no solve in these dumps)
+DUMPS_ALL = DUMPS + ["dump_wetdry_12_tau05.npz", "dump_wetdry_12_edge_depths.npz"]
 RUNS = ["run_flume_21x6_8steps.npz", "run_wetdry_12_4steps.npz"]
 
 
-def gpu_model(case):
+def gpu_model(case, tau=0.0):
     from adh_kraken_b200.capi import SW2Model
     o = OracleModel(case)
     g = SW2Model(case, check_csr=(o.indptr, o.cols))
     d, vx, vy = o.bc_values(case.t0, case.t0 + case.dt)
-    g.set_step(case.dt, d, vx, vy)
+    g.set_step(case.dt, d, vx, vy, tau_temporal=tau)
     return g, o
 
 
-@pytest.mark.parametrize("name", DUMPS)
+def _tau(z):
+    return float(z["tau"]) if "tau" in z.files else 0.0
+
+
+@pytest.mark.parametrize("name", DUMPS_ALL)
 def test_csr_structure_bit_exact(name):
     case, z = load(name)
-    g, _ = gpu_model(case)
+    g, _ = gpu_model(case, _tau(z))
     ip, cl = g.sparsity()
     assert np.array_equal(ip, z["ref_indptr"]) and np.array_equal(cl, z["ref_cols"])
 
 
-@pytest.mark.parametrize("name", DUMPS)
+@pytest.mark.parametrize("name", DUMPS_ALL)
 def test_element_residuals_and_jacobians_bit_exact(name):
     case, z = load(name)
-    g, _ = gpu_model(case)
+    g, _ = gpu_model(case, _tau(z))
     sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
     assert np.array_equal(g.wd_flags(sol, old), z["ref_wd_flag"])
     et, es = g.elem_resid(sol, old, older)
@@ -44,19 +51,19 @@ def test_element_residuals_and_jacobians_bit_exact(name):
     assert np.array_equal(js, z["ref_elem_jac_seg"])
 
 
-@pytest.mark.parametrize("name", DUMPS)
+@pytest.mark.parametrize("name", DUMPS_ALL)
 def test_assembly_bit_exact(name):
     case, z = load(name)
-    g, _ = gpu_model(case)
+    g, _ = gpu_model(case, _tau(z))
     sol, old, older = z["sol"], z["sol_old"], z["sol_older"]
     assert np.array_equal(g.residual(sol, old, older), z["ref_residual"])
     assert np.array_equal(g.jacobian(sol, old, older), z["ref_jac_vals"])
 
 
-@pytest.mark.parametrize("name", DUMPS)
+@pytest.mark.parametrize("name", DUMPS_ALL)
 def test_dirichlet_and_scaling_bit_exact(name):
     case, z = load(name)
-    g, _ = gpu_model(case)
+    g, _ = gpu_model(case, _tau(z))
     vals, res, x, bc, scale = g.prepare_system(z["ref_jac_vals"], z["ref_residual"], np.zeros(3 * case.nnodes),
                                                np.zeros(3 * case.nnodes, np.int32))
     assert np.array_equal(bc, (z["ref_bc_mask"] == 1).astype(np.int32))
@@ -185,3 +192,33 @@ def test_undo_step_retries_the_interval():
     adv = c.advance()
     assert adv["success"] == 1 and adv["substeps"] == 1 and adv["dt_cuts"] == 0
     assert max(rel_err(c.state()[0], sa)) < 1e-10
+
+
+BENCH_OPTS = dict(tol_nonlin=1e-8, tol_nonlin_rel=1e-8, inc_nonlin=1e-6, max_nonlin_it=10, krylov_max_it=20000,
+                  krylov_tol=1e-6, precond=2, krylov_method=1, krylov_restart=50)
+
+
+@pytest.mark.parametrize("mode", ["reference_test", "bench_fast", "bench_plain"])
+def test_config1_flume_100_steps_match_reference(mode):
+    """The CPU-runnable benchmark configuration (101 x 11 flume, 2000 triangles, 100
+    steps of 60 s): every 10th state within 1e-8 relative (h, u, v) of the reference's
+    run, with the reference's absolute Newton test and with the benchmark's options
+    (relative Newton test 1e-8, forcing 1e-6, GMRES(50) + AMG; the fast path in FP32
+    GMRES cycles inside FP64 refinement, the plain path in FP64)."""
+    from adh_kraken_b200.capi import default_opts
+    from adh_kraken_b200.timeloop import SW2Simulation
+    case, z = load("run_flume_101x11_100steps.npz")
+    ref = z["ref_sol_kept"].reshape(-1, 3 * case.nnodes)
+    if mode == "reference_test":
+        opts = default_opts()
+    elif mode == "bench_fast":
+        opts = default_opts(krylov_precision=32, krylov_basis_precision=32, **BENCH_OPTS)
+    else:
+        opts = default_opts(krylov_precision=64, **BENCH_OPTS)
+    sim = SW2Simulation(case, opts=opts)
+    worst = 0.0
+    for k in range(case.nsteps):
+        assert sim.step()["success"], k
+        if (k + 1) % 10 == 0:
+            worst = max(worst, max(rel_err(sim.state()[0], ref[(k + 1) // 10 - 1])))
+    assert worst < 1e-8, worst

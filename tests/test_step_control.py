@@ -24,13 +24,13 @@ class FakeModel:
         self.dt = dt
 
     def step(self, opts=None):
-        from adh_kraken_b200.capi import SW2Error
+        from adh_kraken_b200.capi import ERR_NONFINITE, SW2Error
         assert not self.pending_undo, "a failed step was not undone"
         self.calls.append(self.dt)
         if self.dt > self.dt_ok * (1 + 1e-12):
             self.pending_undo = True
             if self.fail_nonfinite:
-                raise SW2Error("non-finite residual norm during Newton")
+                raise SW2Error("non-finite residual norm during Newton", ERR_NONFINITE)
             return {"success": 0, "newton_its": 10, "krylov_its": 5}
         self.mass += 2.0 * self.dt
         return {"success": 1, "newton_its": 2, "krylov_its": 7}
