@@ -56,7 +56,8 @@ class NewtonStats(C.Structure):
                 ("refine_passes", C.c_int), ("success", C.c_int), ("krylov_breakdowns", C.c_int),
                 ("resid_max", C.c_double), ("resid_l2", C.c_double), ("inc_max", C.c_double),
                 ("initial_resid_max", C.c_double), ("prev_resid_max", C.c_double), ("guess_used", C.c_int),
-                ("initial_resid_l2", C.c_double), ("guess_fallback", C.c_int)]
+                ("initial_resid_l2", C.c_double), ("guess_fallback", C.c_int), ("linear_unconverged", C.c_int),
+                ("tol_used", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -108,7 +108,8 @@ __global__ void k_gm_rowweight(int n, VT* __restrict__ w, const double* __restri
 // accumulators in one thread.  w is read once per group.
 constexpr int kDotGroup = 8;
 template <class VT>
-__global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __restrict__ Vb, size_t ld, int j, GmresDev G) {
+__global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __restrict__ Vb, size_t ld, double* dst,
+                                                 GmresDev G) {
     if (G.state[0]) return;
     __shared__ double sh[8][kDotGroup];
     const int k0 = blockIdx.y * kDotGroup;
@@ -142,18 +143,44 @@ __global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __rest
         if (threadIdx.x < nv) {
             double t = 0;
             for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1) + threadIdx.x);
-            G.H[j * (kGmM + 1) + threadIdx.x] = t;
+            dst[threadIdx.x] = t;
         }
     }
 }
 
-// w -= sum_k h_k v_k ; h_{j+1,j} = ||w|| ; Givens rotation of column j ; convergence test
+// First pass of classical Gram-Schmidt with re-orthogonalisation (CGS2): w -= sum_k h_k v_k, no norm.
 template <class VT>
+__global__ void __launch_bounds__(256) k_gm_sub(int n, int j, VT* __restrict__ Vb, size_t ld, GmresDev G) {
+    if (G.state[0]) return;
+    __shared__ double h[kGmM + 1];
+    for (int k = threadIdx.x; k <= j; k += blockDim.x) h[k] = __ldcg(G.H + j * (kGmM + 1) + k);
+    __syncthreads();
+    VT* w = Vb + (size_t)(j + 1) * ld;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = w[i];
+        int k = 0;
+        for (; k + 8 <= j + 1; k += 8) {
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) x[u] = (double)Vb[(size_t)(k + u) * ld + i];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v -= h[k + u] * x[u];
+        }
+        for (; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
+        w[i] = (VT)v;
+    }
+}
+
+// w -= sum_k h_k v_k ; h_{j+1,j} = ||w|| ; Givens rotation of column j ; convergence test.
+// SECOND: the coefficients come from the re-orthogonalisation pass (G.H2) and are added to
+// those of the first pass (column j of G.H) before the rotations.
+template <class VT, bool SECOND>
 __global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ Vb, size_t ld, GmresDev G) {
     if (G.state[0]) return;
     __shared__ double sh[8];
     __shared__ double h[kGmM + 1];
-    if (threadIdx.x <= j) h[threadIdx.x] = __ldcg(G.H + j * (kGmM + 1) + threadIdx.x);
+    for (int k = threadIdx.x; k <= j; k += blockDim.x)
+        h[k] = SECOND ? __ldcg(G.H2 + k) : __ldcg(G.H + j * (kGmM + 1) + k);
     __syncthreads();
     VT* w = Vb + (size_t)(j + 1) * ld;
     double ss = 0;
@@ -186,6 +213,8 @@ __global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ 
         for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1));
         const double hn = sqrt(t);
         double* col = G.H + j * (kGmM + 1);
+        if (SECOND)
+            for (int k = 0; k <= j; k++) col[k] += G.H2[k];
         for (int k = 0; k < j; k++) {                 // earlier rotations
             const double a = col[k], b = col[k + 1];
             col[k] = G.cs[k] * a + G.sn[k] * b;
@@ -233,7 +262,7 @@ template <class VT>
 __global__ void k_gm_combine(int n, const VT* __restrict__ Vb, size_t ld, VT* __restrict__ out, GmresDev G) {
     __shared__ double y[kGmM];
     const int k = G.state[1];
-    if (threadIdx.x < k) y[threadIdx.x] = G.y[threadIdx.x];
+    for (int t = threadIdx.x; t < k; t += blockDim.x) y[t] = G.y[t];
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = 0;
@@ -244,7 +273,7 @@ __global__ void k_gm_combine(int n, const VT* __restrict__ Vb, size_t ld, VT* __
 
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m) {
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m, bool reorth) {
     const int n = A.n, g = gm_grid(n);
     const int* done = G.state;
     k_gm_start<VT><<<g, 256, 0, st>>>(n, rhs, rw, G);
@@ -257,8 +286,15 @@ void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* 
         precond_apply<VT>(A, P, z, done, st);
         spmv_skip<VT>(A, vals, z, w, done, st);
         k_gm_rowweight<VT><<<g, 256, 0, st>>>(n, w, rw, G);
-        k_gm_dots<VT><<<dim3(g, (j + 1 + kDotGroup - 1) / kDotGroup), 256, 0, st>>>(n, j + 1, Vb, ld, j, G);
-        k_gm_orth<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+        const dim3 dg(g, (j + 1 + kDotGroup - 1) / kDotGroup);
+        k_gm_dots<VT><<<dg, 256, 0, st>>>(n, j + 1, Vb, ld, G.H + (size_t)j * (kGmM + 1), G);
+        if (reorth) {
+            k_gm_sub<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+            k_gm_dots<VT><<<dg, 256, 0, st>>>(n, j + 1, Vb, ld, G.H2, G);
+            k_gm_orth<VT, true><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+        } else {
+            k_gm_orth<VT, false><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
+        }
         k_gm_scale<VT><<<g, 256, 0, st>>>(n, j, Vb, ld, G);
     }
     k_gm_solve<<<1, 32, 0, st>>>(G);
@@ -266,8 +302,8 @@ void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* 
     precond_apply<VT>(A, P, out, nullptr, st);
 }
 template void gmres_cycle<double>(const BlockCSR&, const PrecondOp<double>&, const double*, double*, size_t, double*,
-                                  const double*, double*, const double*, const GmresDev&, cudaStream_t, int);
+                                  const double*, double*, const double*, const GmresDev&, cudaStream_t, int, bool);
 template void gmres_cycle<float>(const BlockCSR&, const PrecondOp<float>&, const float*, float*, size_t, float*,
-                                 const float*, float*, const double*, const GmresDev&, cudaStream_t, int);
+                                 const float*, float*, const double*, const GmresDev&, cudaStream_t, int, bool);
 
 }  // namespace sw2

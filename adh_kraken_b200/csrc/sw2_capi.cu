@@ -88,8 +88,9 @@ struct sw2g_model {
     bool amg_ready = false;
     // restarted GMRES (allocated on first use)
     GmresDev gm{};
-    double* gm_V64 = nullptr;            // [kGmM+1][n] Krylov basis
-    float* gm_V32 = nullptr;             // [kGmM+1][n] FP32 Krylov basis (krylov_basis_precision 32)
+    double* gm_V64 = nullptr;            // [cap+1][n] Krylov basis
+    float* gm_V32 = nullptr;             // [cap+1][n] FP32 Krylov basis (krylov_basis_precision 32)
+    int gm_cap64 = 0, gm_cap32 = 0;      // restart length the bases were allocated for
     cudaGraphExec_t gm_graph_b32 = nullptr;
     int gm_m64 = 0, gm_m32 = 0, gm_mb32 = 0;   // restart length each cycle graph was built for
     double* gm_rw = nullptr;             // [n] row weights 1/s: GMRES minimises the unscaled residual
@@ -112,6 +113,15 @@ static int dalloc(sw2g_model* m, T** p, size_t count) {
     if (e != cudaSuccess) { g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e); *p = nullptr; return SW2G_ERR_NOMEM; }
     m->allocs.push_back((void*)*p);
     return SW2G_OK;
+}
+// frees one allocation made by dalloc
+template <class T>
+static void dfree(sw2g_model* m, T** p) {
+    if (!*p) return;
+    auto it = std::find(m->allocs.begin(), m->allocs.end(), (void*)*p);
+    if (it != m->allocs.end()) m->allocs.erase(it);
+    cudaFree(*p);
+    *p = nullptr;
 }
 template <class T>
 static int upload(sw2g_model* m, T** p, const T* h, size_t count) {
@@ -682,6 +692,8 @@ static int run_bicg(sw2g_model* m, KrylovVecs<VT> V, int precond, cudaGraphExec_
     }
     *iters = m->h_ks->it;
     *status = m->h_ks->status;
+    // status 3: the iteration cap ended the solve before its stopping test held
+    if (*status == 0 && !(m->h_ks->rnorm <= m->h_ks->tol + m->h_ks->bnorm * m->h_ks->rtol)) *status = 3;
     return SW2G_OK;
 }
 
@@ -732,7 +744,7 @@ static int solve64_restarted(sw2g_model* m, double* x, double* b, int max_it, do
             if (!*status) *status = 4;
             break;
         }
-        if (pass > max_restart || *iters >= max_it) break;
+        if (pass > max_restart || *iters >= max_it) { *status = 3; break; }
         prev = rn;
         KrylovVecs<double> V{m->k_xi, m->k_r, m->k_p, m->k_Ap, m->k_q, m->k_s, m->k_As, m->d_t64, m->d_vals, m->d_inv,
                              m->d_lu, m->k_z};
@@ -757,14 +769,31 @@ static int alloc_gmres(sw2g_model* m) {
     if (!m->gm.H) {
         GmresDev& G = m->gm;
         TRY(dalloc(m, &G.H, (size_t)kGmM * (kGmM + 1))); TRY(dalloc(m, &G.cs, kGmM)); TRY(dalloc(m, &G.sn, kGmM));
+        TRY(dalloc(m, &G.H2, kGmM + 1));
         TRY(dalloc(m, &G.g, kGmM + 1)); TRY(dalloc(m, &G.y, kGmM));
         TRY(dalloc(m, &G.partial, (size_t)kMaxBlocks * (kGmM + 1)));
         TRY(dalloc(m, &G.counter, 1)); TRY(dalloc(m, &G.state, 4)); TRY(dalloc(m, &G.scal, 8));
         CK(cudaMemsetAsync(G.counter, 0, sizeof(unsigned int), m->st));
     }
-    if (!m->gm_V64) TRY(dalloc(m, &m->gm_V64, (size_t)(kGmM + 1) * m->n));
     if (!m->gm_rw) TRY(dalloc(m, &m->gm_rw, (size_t)m->n));
     return SW2G_OK;
+}
+
+// Krylov basis of mres + 1 vectors, grown when a longer restart is asked for
+template <class T>
+static int gmres_basis(sw2g_model* m, T** V, int* cap, int mres) {
+    if (*V && *cap >= mres) return SW2G_OK;
+    CK(cudaStreamSynchronize(m->st));
+    dfree(m, V);
+    TRY(dalloc(m, V, (size_t)(mres + 1) * m->n));
+    *cap = mres;
+    return SW2G_OK;
+}
+
+// classical Gram-Schmidt with one re-orthogonalisation pass (SW2G_GM_REORTH=1; diagnostic switch)
+static bool gm_reorth() {
+    static const bool on = getenv("SW2G_GM_REORTH") != nullptr && getenv("SW2G_GM_REORTH")[0] == '1';
+    return on;
 }
 
 // FP32 cycle: FP32 basis, FP32 matrix and FP32 preconditioner on the FP32 right-hand side f_b; the
@@ -779,7 +808,7 @@ static int gmres_graph32(sw2g_model* m, cudaGraphExec_t* graph, int* built_m, in
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
     gmres_cycle<float>(m->B, op, m->f_vals, m->gm_V32, (size_t)m->n, m->f_z, m->f_b, m->f_x, m->gm_rw, m->gm, m->st,
-                       mres);
+                       mres, gm_reorth());
     cudaError_t e1 = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
@@ -802,7 +831,7 @@ static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, int* built_m, bool
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
     gmres_cycle<double>(m->B, op, m->d_vals, m->gm_V64, (size_t)m->n, m->k_z, m->d_t64, m->k_xi, m->gm_rw, m->gm,
-                        m->st, mres);
+                        m->st, mres, gm_reorth());
     cudaError_t e1 = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
@@ -851,9 +880,16 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
     }
     const bool basis32 = mixed && o.krylov_basis_precision == 32;
     if (basis32) {
-        if (!m->gm_V32) TRY(dalloc(m, &m->gm_V32, (size_t)(kGmM + 1) * n));
+        if (!m->gm_V32 || m->gm_cap32 < mres) {
+            TRY(gmres_basis(m, &m->gm_V32, &m->gm_cap32, mres));
+            m->gm_mb32 = -1;   // the cycle graph holds the old basis address
+        }
         TRY(gmres_graph32(m, &m->gm_graph_b32, &m->gm_mb32, o.precond, mres));
     } else {
+        if (!m->gm_V64 || m->gm_cap64 < mres) {
+            TRY(gmres_basis(m, &m->gm_V64, &m->gm_cap64, mres));
+            m->gm_m32 = m->gm_m64 = -1;
+        }
         TRY(gmres_graph(m, mixed ? &m->gm_graph32 : &m->gm_graph64, mixed ? &m->gm_m32 : &m->gm_m64, mixed, o.precond,
                         mres));
     }
@@ -892,9 +928,24 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         if (!(rn > target)) break;
         if (pass > 0) {
             stall = (rn > 0.99 * prev) ? stall + 1 : 0;
-            if (stall >= 3) { *status = 4; break; }
+            if (stall >= 3) {
+                *status = 4;
+                if (trace) {   // where the stalled linear residual sits (largest unscaled entries)
+                    std::vector<double> t(n), sc(n);
+                    CK(cudaMemcpyAsync(t.data(), m->d_t64, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+                    CK(cudaMemcpyAsync(sc.data(), m->d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost, m->st));
+                    CK(cudaStreamSynchronize(m->st));
+                    std::vector<int> idx(n);
+                    for (int i = 0; i < n; i++) { idx[i] = i; t[i] = fabs(t[i] / sc[i]); }
+                    std::partial_sort(idx.begin(), idx.begin() + 8, idx.end(), [&](int a, int b) { return t[a] > t[b]; });
+                    fprintf(stderr, "gmres stalled; largest |r|:");
+                    for (int k = 0; k < 8; k++) fprintf(stderr, " %d:%.2e", idx[k], t[idx[k]]);
+                    fprintf(stderr, "\n");
+                }
+                break;
+            }
         }
-        if (*iters >= o.krylov_max_it) break;
+        if (*iters >= o.krylov_max_it) { *status = 3; break; }
         prev = rn;
         double rtol = 0.5 * target / rn;         // the cycle's own 2-norm estimate of the reduction still needed
         if (rtol < (basis32 ? 1e-5 : 1e-12)) rtol = basis32 ? 1e-5 : 1e-12;   // FP32 resolves no more per cycle
@@ -973,7 +1024,8 @@ static int solve32(sw2g_model* m, double* x, double* b, const sw2g_newton_opts& 
             break;
         }
         if (!std::isfinite(rn)) { *status = 2; break; }
-        if (!(rn > o.krylov_tol + bnorm * o.krylov_tol) || pass == o.max_refine) break;
+        if (!(rn > o.krylov_tol + bnorm * o.krylov_tol)) break;
+        if (pass == o.max_refine) { if (!*status) *status = 3; break; }
         prev_rn = rn;
         {
             ProfScope ps(m, 4, 1);
@@ -1101,7 +1153,7 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
     sw2g_newton_opts o = o_in;   // the step's effective options
     // relative test: against the previous-step state's residual, the same reference with or without a guess
     if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = o_in.tol_nonlin_rel * st.prev_resid_max;
-    int it = 0; bool ok = true, keep, lin_stalled = false;
+    int it = 0; bool ok = true, keep, lin_ok = true;
     do {
         TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
         CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
@@ -1145,20 +1197,25 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
             static const bool trace_nf = getenv("SW2G_TRACE_NEWTON") != nullptr;
             if (trace_nf) debug_nonfinite(m);
         }
-        // a failed linear solve that left a zero increment must not read as an increment below inc_nonlin
-        lin_stalled = (lin_status != 0 && !(imax > 0.0));
+        // The increment test stands for convergence only when the linear solve reached its target: with
+        // the reference's exact LU (bcgstab_solver.c:371-420) a small increment means Newton converged,
+        // with an iterative solve that stopped early it may only mean the solve stalled.
+        lin_ok = (lin_status == 0);
+        if (!lin_ok) st.linear_unconverged++;
         st.linesearch_cuts += cuts;
         it++;
         static const bool trace = getenv("SW2G_TRACE_NEWTON") != nullptr;   // diagnostic: Newton history on stderr
         if (trace)
             fprintf(stderr, "newton it %d krylov %d status %d refine %d resid_max %.3e resid_l2 %.3e inc_max %.3e cuts %d\n",
                     it, kit, kst, passes, rmax, rl2, imax, cuts);
-        keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && imax > o.inc_nonlin;
+        keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && (imax > o.inc_nonlin || !lin_ok);
     } while (keep);
     st.newton_its = it;
     st.resid_max = rmax; st.resid_l2 = rl2; st.inc_max = imax;
-    // a linear solve that made no progress leaves a zero increment, which must not read as convergence
-    st.success = !((rmax > o.tol_nonlin && (imax > o.inc_nonlin || lin_stalled)) || rmax >= 1.0E+20 || !ok);
+    st.tol_used = o.tol_nonlin;
+    // fe_newton.c:870-871 (success unless max|R| > tol and the increment > inc_nonlin), with the
+    // increment test counted only after a linear solve that reached its target
+    st.success = ok && rmax < 1.0E+20 && (!(rmax > o.tol_nonlin) || (!(imax > o.inc_nonlin) && lin_ok));
     if (!st.success) {   // fe_newton.c:887-890: reset to the old values
         CK(cudaMemcpyAsync(m->d_sol, m->d_sol_old, sizeof(double) * n, cudaMemcpyDeviceToDevice, m->st));
         launch_masked_copy(n, m->d_bc_mask, m->d_dirichlet, m->d_sol, m->st);
@@ -1372,6 +1429,7 @@ static int newton_with_fallback(sw2g_model* m, const sw2g_newton_opts& o, sw2g_n
         rc = newton_device(m, o2, &b);
         b.newton_its += a.newton_its; b.krylov_its += a.krylov_its; b.linesearch_cuts += a.linesearch_cuts;
         b.refine_passes += a.refine_passes; b.krylov_breakdowns += a.krylov_breakdowns;
+        b.linear_unconverged += a.linear_unconverged;
         b.guess_fallback = 1;
         a = b;
     }

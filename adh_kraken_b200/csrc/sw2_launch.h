@@ -180,10 +180,11 @@ template <class VT>
 void precond_apply(const BlockCSR& A, const PrecondOp<VT>& P, VT* y, const int* skip, cudaStream_t st);
 
 // ---- restarted GMRES(m) cycle (gmres_kernels.cu)
-constexpr int kGmM = 50;                // largest Krylov dimension of one cycle (buffers, register arrays)
+constexpr int kGmM = 200;               // largest Krylov dimension of one cycle (Hessenberg and partial buffers)
 constexpr int kGmDefault = 30;          // default restart length
 struct GmresDev {                       // device buffers of one cycle
     double* H = nullptr;                // [kGmM][kGmM+1] Hessenberg columns (rotated in place)
+    double* H2 = nullptr;               // [kGmM+1] coefficients of the re-orthogonalisation pass
     double* cs = nullptr; double* sn = nullptr;   // [kGmM] Givens rotations
     double* g = nullptr;                // [kGmM+1] rotated right-hand side
     double* y = nullptr;                // [kGmM] least-squares solution
@@ -196,7 +197,7 @@ struct GmresDev {                       // device buffers of one cycle
 // residual 2-norm; Vb holds kGmM+1 vectors of stride ld
 template <class VT>
 void gmres_cycle(const BlockCSR& A, const PrecondOp<VT>& P, const VT* vals, VT* Vb, size_t ld, VT* z, const VT* rhs,
-                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m);
+                 VT* out, const double* rw, const GmresDev& G, cudaStream_t st, int m, bool reorth);
 // rw_i = 1 / s_i (weights that make a scaled system's residual the unscaled one)
 void launch_inv_scale(int n, const double* scale, double* rw, cudaStream_t st);
 template <class VT>

@@ -159,15 +159,15 @@ class SW2Simulation:
         steps of the reduced size.  The reference instead ends its time loop at the
         first failure (src/timeloop/time_loop.c:37).  Gives up after max_cuts
         reductions (success 0, the state and the clock at the last good substep).
-        ``before_attempt(sim)``, when given, runs before every Newton solve (e.g. to
-        set an initial guess).  Failed attempts are undone before anything else runs:
+        ``before_attempt(sim, dt)``, when given, runs before every Newton solve (e.g.
+        to set an initial guess for a step of that dt).  Failed attempts are undone before anything else runs:
         the clock never moves for them and the mass log never sees them."""
         target = self.t + self.case.dt
         dt, cuts, subs, failed = self.case.dt, 0, [], []
         while self.t + NOT_QUITE_SMALL * self.case.dt < target:
             h = min(dt, target - self.t)
             if before_attempt is not None:
-                before_attempt(self)
+                before_attempt(self, h)
             st, t_new = self._attempt(opts, h)
             if st["success"]:
                 self._record(st, t_new, h, moved=True)
@@ -183,7 +183,8 @@ class SW2Simulation:
         ok = cuts <= max_cuts
         out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts,
                "newton_its": sum(s["newton_its"] for s in subs + failed),
-               "krylov_its": sum(s["krylov_its"] for s in subs + failed)}
+               "krylov_its": sum(s["krylov_its"] for s in subs + failed),
+               "linear_unconverged": sum(s.get("linear_unconverged", 0) for s in subs + failed)}
         if subs:
             last = subs[-1]
             for k in ("resid_max", "inc_max", "tol_used"):

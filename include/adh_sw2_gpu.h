@@ -67,7 +67,7 @@ typedef struct {
     int krylov_basis_precision; /* GMRES with krylov_precision 32: 64 (default) keeps the Krylov basis, the SpMV
                                  and the Gram-Schmidt in FP64 around the FP32 preconditioner; 32 runs the whole
                                  cycle in FP32, each cycle refined from the FP64 residual */
-    int krylov_restart;       /* GMRES restart length, 1..50 (default 30) */
+    int krylov_restart;       /* GMRES restart length, 1..200 (default 30); the basis holds restart+1 vectors */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's
@@ -87,7 +87,8 @@ typedef struct {
     int krylov_its;           /* Krylov (BiCGStab or GMRES) iterations summed over the step */
     int linesearch_cuts;      /* line-search halvings summed over the step */
     int refine_passes;        /* FP64 refinement passes (32-bit mode) */
-    int success;              /* fe_newton's TRUE/FALSE */
+    int success;              /* fe_newton's TRUE/FALSE: max|R| <= tolerance, or the increment max-norm <=
+                                 inc_nonlin after a linear solve that reached its target */
     int krylov_breakdowns;    /* Krylov solves that stopped on a zero/non-finite denominator */
     double resid_max;         /* final max |R| over non-Dirichlet dofs */
     double resid_l2;          /* final sqrt(sum R^2)/ndofs */
@@ -98,6 +99,10 @@ typedef struct {
     double initial_resid_l2;  /* sqrt(sum R^2)/ndofs at the initial guess */
     int guess_fallback;       /* 1: Newton from the guess failed and was repeated from the previous step
                                  (the counts above include both attempts) */
+    int linear_unconverged;   /* Newton iterations whose linear solve stopped before its target (iteration
+                                 cap, stall, breakdown); their increment test does not count as convergence */
+    double tol_used;          /* the Newton residual tolerance applied (tol_nonlin, or tol_nonlin_rel times
+                                 max|R(sol_old)|) */
 } sw2g_newton_stats;
 
 /* --- lifetime ------------------------------------------------------------ */

@@ -65,6 +65,30 @@ def read_records(path):
     return out
 
 
+class HarnessRun:
+    """One harness run in the background (a subprocess): start() returns at once,
+    wait() returns its records.  Used where the reference's CPU run overlaps other work."""
+
+    def __init__(self, mode, case, extra=(), binary=HARNESS):
+        if not harness_available(binary):
+            raise RuntimeError(f"reference harness not built ({binary})")
+        self.td = tempfile.TemporaryDirectory()
+        cpath = os.path.join(self.td.name, "case.bin")
+        self.opath = os.path.join(self.td.name, "out.bin")
+        write_case(case, cpath)
+        self.p = subprocess.Popen([binary, mode, cpath, self.opath, *map(str, extra)], stdout=subprocess.DEVNULL,
+                                  stderr=subprocess.PIPE, cwd=self.td.name)
+
+    def wait(self, timeout=3600):
+        _, err = self.p.communicate(timeout=timeout)
+        try:
+            if self.p.returncode != 0:
+                raise RuntimeError(f"harness failed ({self.p.returncode}): {err.decode()[-2000:]}")
+            return read_records(self.opath)
+        finally:
+            self.td.cleanup()
+
+
 def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=None, env=None, timeout=3600,
                 in_path=None, binary=HARNESS):
     if not harness_available(binary):

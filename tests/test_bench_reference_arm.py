@@ -27,6 +27,7 @@ def test_reference_arm_json_line(monkeypatch):
     assert out["impl"] == "reference" and out["metric"] == bench.METRIC and out["unit"] == bench.UNIT
     assert out["value"] > 0 and out["steps"] == 2 and out["warmup"] == 1
     assert out["cpu_baseline"]["value"] == out["value"] and out["cpu_baseline"]["cores"] == 1
-    assert out["cpu_baseline"]["kind"] == "reference" and "2 timed steps" in out["cpu_baseline"]["sample"]
+    assert out["cpu_baseline"]["kind"] == "reference" and "steps 2..3" in out["cpu_baseline"]["sample"]
+    assert "lower bound" in out["cpu_baseline"]["sample"]
     assert out["e2e"] == {"value": out["value"], "unit": out["unit"], "h2d_bytes_per_step": 0,
                           "d2h_bytes_per_step": 0}
