@@ -25,7 +25,7 @@ EXPORTED = [
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
     "sw2g_assemble_residual_noalloc", "sw2g_grid_mass", "sw2g_undo_step",
-    "sw2g_assemble_residual_wd", "sw2g_assemble_jacobian_wd",
+    "sw2g_assemble_residual_wd", "sw2g_assemble_jacobian_wd", "sw2g_precond_info",
     # include/adh_sw2_gnn.h (learned initial guess)
     "sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
     "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj",
@@ -42,7 +42,8 @@ class NewtonOpts(C.Structure):
                 ("max_linesearch_cuts", C.c_int), ("krylov_max_it", C.c_int), ("krylov_tol", C.c_double),
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
                 ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int),
-                ("tol_nonlin_rel", C.c_double), ("krylov_basis_precision", C.c_int), ("krylov_restart", C.c_int)]
+                ("tol_nonlin_rel", C.c_double), ("krylov_basis_precision", C.c_int), ("krylov_restart", C.c_int),
+                ("amg_chunks", C.c_int)]
 
 PC_BLOCK_JACOBI = 0
 PC_BILU0 = 1
@@ -287,13 +288,21 @@ class SW2Model:
         self._check(lib().sw2g_get_profile(self.h, _d(ms), n.ctypes.data_as(C.POINTER(C.c_longlong))))
         return ms, n
 
+    def precond_info(self):
+        """The AMG's chunk corrections at the last preconditioner set-up (sw2g_precond_info)."""
+        info = np.zeros(5, np.int64)
+        self._check(lib().sw2g_precond_info(self.h, info.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return dict(zip(("flagged_nodes", "chunks", "chunk_nodes", "inverse_entries", "singular_chunks"),
+                        (int(v) for v in info)))
+
     def reset_profile(self):
         self._check(lib().sw2g_reset_profile(self.h))
 
     def time_kernel(self, which, reps=20):
         """(mean ms per launch, algorithmic bytes per launch) of kernel family `which`:
         0 FP64 SpMV, 1 FD Jacobian, 2 element residual, 3 Jacobian gather, 4 AMG smoothing sweep (FP64),
-        5 AMG smoothing sweep (FP32)."""
+        5 AMG smoothing sweep (FP32), 6 FP32 V-cycle, 7 FP32 SpMV, 8 one FP32 GMRES cycle (second value: its
+        iterations), 9 the AMG chunk corrections (FP32)."""
         ms, by = C.c_double(), C.c_double()
         self._check(lib().sw2g_time_kernel(self.h, int(which), int(reps), C.byref(ms), C.byref(by)))
         return ms.value, by.value

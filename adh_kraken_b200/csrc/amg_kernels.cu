@@ -88,7 +88,10 @@ __device__ __forceinline__ bool inv3(const double* a, double* o) {
 // ||D^-1||_inf * max_v off_v exceeds kAmgGainMax (nearly singular blocks, e.g.
 // at the inflow boundary) gets that for all three rows.  off_v = sum of |a| of
 // row v outside the diagonal block.
-__device__ __forceinline__ void l1_block_inverse(const double* a_in, const double* off, double* o) {
+// Returns true when the block the smoother uses is much weaker than the plain inverse
+// (sum of |entries| below kPatchFlagRatio of it, or no plain inverse at all): block-Jacobi
+// barely moves such a node, so the chunk correction takes it over.
+__device__ __forceinline__ bool l1_block_inverse(const double* a_in, const double* off, double* o) {
     double a[9];
 #pragma unroll
     for (int e = 0; e < 9; e++) a[e] = a_in[e];
@@ -102,15 +105,22 @@ __device__ __forceinline__ void l1_block_inverse(const double* a_in, const doubl
         for (int v = 0; v < 3; v++) gain = fmax(gain, (fabs(o[3 * v]) + fabs(o[3 * v + 1]) + fabs(o[3 * v + 2])) * offmax);
     }
     if (!ok || gain > kAmgGainMax) { fix[0] = fix[1] = fix[2] = true; any = true; }
-    if (!any) return;
+    if (!any) return false;
+    double plain = 0.0;
+#pragma unroll
+    for (int e = 0; e < 9; e++) plain += fabs(o[e]);
 #pragma unroll
     for (int v = 0; v < 3; v++)
         if (fix[v]) a[4 * v] += (a[4 * v] >= 0.0 ? off[v] : -off[v]);
     inv3(a, o);
+    double fixed = 0.0;
+#pragma unroll
+    for (int e = 0; e < 9; e++) fixed += fabs(o[e]);
+    return !ok || fixed < kPatchFlagRatio * plain;
 }
 
 // level 0: diagonal blocks and off-block row sums read from the reference CSR
-__global__ void k_amg_dinv0(BlockCSR A, const double* __restrict__ vals, double* __restrict__ dinv) {
+__global__ void k_amg_dinv0(BlockCSR A, const double* __restrict__ vals, double* __restrict__ dinv, int* __restrict__ flag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nnodes) return;
     const int rs = A.indptr[3 * i], len = A.indptr[3 * i + 1] - rs;
@@ -123,7 +133,8 @@ __global__ void k_amg_dinv0(BlockCSR A, const double* __restrict__ vals, double*
             else off[v] += fabs(row[q]);
         }
     }
-    l1_block_inverse(blk, off, dinv + 9 * (size_t)i);
+    const bool weak = l1_block_inverse(blk, off, dinv + 9 * (size_t)i);
+    if (flag) flag[i] = weak ? 1 : 0;
 }
 
 // coarse levels (block CSR)
@@ -329,9 +340,189 @@ __global__ void k_amg_copy(int n, const VT* __restrict__ a, VT* __restrict__ b, 
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
+// ---------------------------------------------------------------- chunk corrections (level 0)
+// One CTA per chunk (grid-stride): the chunk's dense block of the scaled level-0 matrix
+// (its nodes' rows and columns; couplings to nodes outside the chunk are left out) is
+// inverted by Gauss-Jordan elimination with partial pivoting in shared memory, and the
+// rows of the chunk's own dofs (own nodes come first) are written in FP64 and FP32.  A
+// zero pivot leaves the chunk's rows at zero (no correction) and is counted.
+constexpr int kPatchMaxDof = 3 * kPatchMaxNodes;
+__global__ void __launch_bounds__(256) k_patch_invert(BlockCSR A, PatchDev P, const double* __restrict__ vals,
+                                                      int nchunks) {
+    extern __shared__ double sm[];                 // [m * m], m = 3 * chunk nodes
+    __shared__ int nodes[kPatchMaxNodes];
+    __shared__ int piv[kPatchMaxDof];
+    __shared__ double colk[kPatchMaxDof];
+    __shared__ int s_p, s_bad;
+    __shared__ double s_pinv;
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const int p0 = P.chunk_ptr[c], ne = P.chunk_ptr[c + 1] - p0, own = P.own_cnt[c];
+        const int m = 3 * ne;
+        for (int t = threadIdx.x; t < ne; t += blockDim.x) nodes[t] = P.ext_node[p0 + t];
+        for (int t = threadIdx.x; t < m * m; t += blockDim.x) sm[t] = 0.0;
+        if (threadIdx.x == 0) s_bad = 0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < ne * 32; t += blockDim.x) {   // (chunk node, neighbour slot)
+            const int ia = t >> 5, q = t & 31;
+            const int a = nodes[ia];
+            const int s0 = A.bptr[a], deg = A.bptr[a + 1] - s0;
+            if (q >= deg) continue;
+            const int b = A.bcol[s0 + q];
+            int ib = -1;
+            for (int k = 0; k < ne; k++)
+                if (nodes[k] == b) { ib = k; break; }
+            if (ib < 0) continue;
+            const int rs = A.indptr[3 * a], len = A.indptr[3 * a + 1] - rs;
+#pragma unroll
+            for (int v = 0; v < 3; v++)
+#pragma unroll
+                for (int w = 0; w < 3; w++) sm[(3 * ia + v) * m + 3 * ib + w] = vals[rs + v * len + 3 * q + w];
+        }
+        __syncthreads();
+        for (int k = 0; k < m; k++) {
+            if (threadIdx.x < 32) {                    // pivot: largest |a_ik|, i >= k (lowest index on ties)
+                double best = -1.0;
+                int bi = k;
+                for (int i = k + threadIdx.x; i < m; i += 32) {
+                    const double v = fabs(sm[i * m + k]);
+                    if (v > best) { best = v; bi = i; }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+                }
+                if (threadIdx.x == 0) {
+                    s_p = bi; piv[k] = bi;
+                    if (!(best > 1e-300) || !isfinite(best)) s_bad = 1;
+                }
+            }
+            __syncthreads();
+            if (s_bad) break;
+            const int p = s_p;
+            if (p != k)
+                for (int j = threadIdx.x; j < m; j += blockDim.x) {
+                    const double t0 = sm[k * m + j];
+                    sm[k * m + j] = sm[p * m + j];
+                    sm[p * m + j] = t0;
+                }
+            __syncthreads();
+            if (threadIdx.x == 0) s_pinv = 1.0 / sm[k * m + k];
+            __syncthreads();
+            const double pinv = s_pinv;
+            for (int j = threadIdx.x; j < m; j += blockDim.x) sm[k * m + j] = (j == k) ? pinv : sm[k * m + j] * pinv;
+            for (int i = threadIdx.x; i < m; i += blockDim.x) colk[i] = sm[i * m + k];
+            __syncthreads();
+            for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+                const int i = t / m, j = t - i * m;
+                if (i == k) continue;
+                sm[t] = (j == k) ? -colk[i] * pinv : sm[t] - colk[i] * sm[k * m + j];
+            }
+            __syncthreads();
+        }
+        const int ro = 3 * own;
+        double* R = P.r64 + P.rofs[c];
+        float* R32 = P.r32 + P.rofs[c];
+        if (s_bad) {
+            for (int t = threadIdx.x; t < ro * m; t += blockDim.x) { R[t] = 0.0; R32[t] = 0.0f; }
+            if (threadIdx.x == 0) atomicAdd(P.failed, 1);
+            __syncthreads();
+            continue;
+        }
+        for (int k = m - 1; k >= 0; k--) {           // undo the row interchanges on the columns
+            const int p = piv[k];
+            if (p != k)
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    const double t0 = sm[i * m + k];
+                    sm[i * m + k] = sm[i * m + p];
+                    sm[i * m + p] = t0;
+                }
+            __syncthreads();
+        }
+        for (int t = threadIdx.x; t < ro * m; t += blockDim.x) { R[t] = sm[t]; R32[t] = (float)sm[t]; }
+        __syncthreads();
+    }
+}
+
+// e = b - A x at every chunk node (entries of all chunks; a node in several chunks is
+// evaluated once per chunk)
+template <class VT>
+__global__ void __launch_bounds__(256) k_patch_resid(BlockCSR A, const VT* __restrict__ vals, const VT* __restrict__ b,
+                                                     const VT* __restrict__ x, PatchDev P, VT* __restrict__ e,
+                                                     const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int ne = P.counts[1];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x) {
+        const int a = P.ext_node[t];
+        const int rs = A.indptr[3 * a], len = A.indptr[3 * a + 1] - rs;
+        const int s0 = A.bptr[a], deg = A.bptr[a + 1] - s0;
+        double y0 = 0, y1 = 0, y2 = 0;
+        for (int j = 0; j < deg; j++) {
+            const int c = A.bcol[s0 + j];
+            const double x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
+            const VT* v0 = vals + rs + 3 * j;
+            y0 += (double)v0[0] * x0 + (double)v0[1] * x1 + (double)v0[2] * x2;
+            const VT* v1 = v0 + len;
+            y1 += (double)v1[0] * x0 + (double)v1[1] * x1 + (double)v1[2] * x2;
+            const VT* v2 = v1 + len;
+            y2 += (double)v2[0] * x0 + (double)v2[1] * x1 + (double)v2[2] * x2;
+        }
+        e[3 * t] = (VT)((double)b[3 * a] - y0);
+        e[3 * t + 1] = (VT)((double)b[3 * a + 1] - y1);
+        e[3 * t + 2] = (VT)((double)b[3 * a + 2] - y2);
+    }
+}
+
+template <class VT> struct PatchBuf;
+template <> struct PatchBuf<double> {
+    static const double* r(const PatchDev& P) { return P.r64; }
+    static double* e(const PatchDev& P) { return P.e64; }
+};
+template <> struct PatchBuf<float> {
+    static const float* r(const PatchDev& P) { return P.r32; }
+    static float* e(const PatchDev& P) { return P.e32; }
+};
+
+// x[own dofs of chunk c] += R_c e_c; the own nodes of different chunks are disjoint
+template <class VT>
+__global__ void __launch_bounds__(256) k_patch_apply(PatchDev P, const VT* __restrict__ R, const VT* __restrict__ e,
+                                                     VT* __restrict__ x, const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int nch = P.counts[0];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+        const int p0 = P.chunk_ptr[c], m = 3 * (P.chunk_ptr[c + 1] - p0), ro = 3 * P.own_cnt[c];
+        const VT* Rc = R + P.rofs[c];
+        const VT* ec = e + 3 * (size_t)p0;
+        for (int i = warp; i < ro; i += nw) {
+            double acc = 0.0;
+            for (int j = lane; j < m; j += 32) acc += (double)Rc[(size_t)i * m + j] * (double)ec[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                const int node = P.ext_node[p0 + i / 3];
+                const int d = 3 * node + i % 3;
+                x[d] = (VT)((double)x[d] + acc);
+            }
+        }
+    }
+}
+
+void patch_invert(const BlockCSR& A, const PatchDev& P, const double* vals, int nchunks, cudaStream_t st) {
+    if (nchunks <= 0) return;
+    static bool attr = false;
+    const int smem = kPatchMaxDof * kPatchMaxDof * (int)sizeof(double);
+    if (!attr) {
+        cudaFuncSetAttribute(k_patch_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    k_patch_invert<<<P.grid, 256, smem, st>>>(A, P, vals, nchunks);
+}
+
 // ---------------------------------------------------------------- host side
 void amg_setup(const BlockCSR& A, const AmgHost& H, const AssemblyMaps& maps, const double* vals, cudaStream_t st) {
-    k_amg_dinv0<<<nb(A.nnodes, 128), 128, 0, st>>>(A, vals, H.dinv0_64);
+    k_amg_dinv0<<<nb(A.nnodes, 128), 128, 0, st>>>(A, vals, H.dinv0_64, H.patch.flag);
     for (int l = 1; l < H.nlev; l++) {
         const AmgLevel& C = H.lev[l];
         const AmgLink& K = H.link[l - 1];
@@ -366,6 +557,9 @@ static void smooth_or_resid(const BlockCSR& A, const AmgLevel& L, int l, const V
 
 // one V-cycle at level l: x <- V(b); level 0 uses the CSR values passed in
 template <class VT>
+void amg_patch_correct(const BlockCSR& A, const AmgHost& H, const VT* vals0, const VT* b, VT* y, const int* skip,
+                       cudaStream_t st);
+template <class VT>
 static void vcycle(const BlockCSR& A, const AmgHost& H, int l, const VT* vals0, const VT* b, VT* x, const int* skip,
                    cudaStream_t st) {
     const AmgLevel& L = H.lev[l];
@@ -386,6 +580,7 @@ static void vcycle(const BlockCSR& A, const AmgHost& H, int l, const VT* vals0, 
         smooth_or_resid<VT>(A, L, l, vals0, dinv, b, cur, nxt, false, skip, st);
         cur = nxt;
     }
+    if (l == 0 && H.patch.mode == 2) amg_patch_correct<VT>(A, H, vals0, b, cur, skip, st);
     // coarse correction
     const AmgLevel& C = H.lev[l + 1];
     const AmgLink& K = H.link[l];
@@ -399,6 +594,7 @@ static void vcycle(const BlockCSR& A, const AmgHost& H, int l, const VT* vals0, 
         smooth_or_resid<VT>(A, L, l, vals0, dinv, b, cur, nxt, false, skip, st);
         cur = nxt;
     }
+    if (l == 0 && H.patch.mode == 2) amg_patch_correct<VT>(A, H, vals0, b, cur, skip, st);
     if (cur != x) k_amg_copy<VT><<<nb(3L * n, 256), 256, 0, st>>>(3 * n, cur, x, skip);
 }
 
@@ -415,11 +611,28 @@ void amg_smooth0_once32(const BlockCSR& A, const AmgHost& H, const float* vals, 
 }
 
 template <class VT>
+void amg_patch_correct(const BlockCSR& A, const AmgHost& H, const VT* vals0, const VT* b, VT* y, const int* skip,
+                       cudaStream_t st);
+template <class VT>
 void amg_apply(const BlockCSR& A, const AmgHost& H, const VT* vals0, VT* y, const int* skip, cudaStream_t st) {
     VT* b0 = AmgBuf<VT>::b(H.lev[0]);
     k_amg_copy<VT><<<1184, 256, 0, st>>>(3 * A.nnodes, y, b0, skip);
     vcycle<VT>(A, H, 0, vals0, b0, y, skip, st);
+    if (H.patch.mode == 1) amg_patch_correct<VT>(A, H, vals0, b0, y, skip, st);
 }
+
+template <class VT>
+void amg_patch_correct(const BlockCSR& A, const AmgHost& H, const VT* vals0, const VT* b, VT* y, const int* skip,
+                       cudaStream_t st) {
+    if (!H.patch.flag) return;   // chunk corrections on the flagged nodes (counts read on the device)
+    const PatchDev& P = H.patch;
+    k_patch_resid<VT><<<P.grid, 256, 0, st>>>(A, vals0, b, y, P, PatchBuf<VT>::e(P), skip);
+    k_patch_apply<VT><<<P.grid, 256, 0, st>>>(P, PatchBuf<VT>::r(P), PatchBuf<VT>::e(P), y, skip);
+}
+template void amg_patch_correct<double>(const BlockCSR&, const AmgHost&, const double*, const double*, double*,
+                                        const int*, cudaStream_t);
+template void amg_patch_correct<float>(const BlockCSR&, const AmgHost&, const float*, const float*, float*,
+                                       const int*, cudaStream_t);
 template void amg_apply<double>(const BlockCSR&, const AmgHost&, const double*, double*, const int*, cudaStream_t);
 template void amg_apply<float>(const BlockCSR&, const AmgHost&, const float*, float*, const int*, cudaStream_t);
 

@@ -42,6 +42,7 @@ extern "C" const char* sw2g_last_error(void) { return g_err.c_str(); }
 #define TRY(x) do { int r_ = (x); if (r_ != SW2G_OK) return r_; } while (0)
 
 static const int kChunk = 8;   // BiCGStab iterations per graph replay
+static const double kPatchTileEdges = 7.0;   // tile side of the AMG chunk corrections, in mean edge lengths
 
 struct ProfRec { int cls; cudaEvent_t a, b; };
 
@@ -96,6 +97,14 @@ struct sw2g_model {
     double* gm_rw = nullptr;             // [n] row weights 1/s: GMRES minimises the unscaled residual
     cudaGraphExec_t gm_graph64 = nullptr, gm_graph32 = nullptr;
     std::vector<int> h_bptr, h_bcol;   // node graph, kept for the AMG set-up
+    // chunk corrections of the AMG (built every Newton iteration from the flagged nodes)
+    std::vector<long long> h_tile;     // [V] tile of each node (squares of kPatchTileEdges mean edge lengths)
+    int* h_pflag = nullptr;            // pinned [V] flags read back
+    int *h_cptr = nullptr, *h_cown = nullptr, *h_cnode = nullptr;   // pinned staging of the chunk build
+    long long* h_crofs = nullptr;
+    int pcap_chunks = 0, pcap_entries = 0; long long pcap_r = 0;
+    int p_nchunks = 0, p_nentries = 0, p_nflag = 0;
+    long long p_rtot = 0;
     StepParams P{};
     MeshView M{}; AssemblyMaps A{}; BlockCSR B{};
     // profiling
@@ -194,6 +203,7 @@ extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->tol_nonlin_rel = 0.0;
     o->krylov_basis_precision = 64;
     o->krylov_restart = 30;
+    o->amg_chunks = 0;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -244,6 +254,20 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         double d = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]));
         if (!(d > 1e-6)) { g_err = "sw2g_create: zero-length boundary segment"; return fail(SW2G_ERR_MESH); }
         sdj[k] = d; snx[k] = (b[1] - a[1]) / d; sny[k] = -(b[0] - a[0]) / d;
+    }
+
+    // --- tiles of the AMG chunk corrections: squares of kPatchTileEdges mean edge lengths
+    {
+        double area = 0.0, xmin = 1e300, ymin = 1e300;
+        for (int e = 0; e < T; e++) area += dj[e];
+        for (int i = 0; i < V; i++) { xmin = std::min(xmin, mesh->xyz[3 * (size_t)i]); ymin = std::min(ymin, mesh->xyz[3 * (size_t)i + 1]); }
+        const double edge = sqrt(2.0 * area / T), side = kPatchTileEdges * edge;
+        m->h_tile.resize(V);
+        for (int i = 0; i < V; i++) {
+            const long long tx = (long long)floor((mesh->xyz[3 * (size_t)i] - xmin) / side);
+            const long long ty = (long long)floor((mesh->xyz[3 * (size_t)i + 1] - ymin) / side);
+            m->h_tile[i] = tx * 4000000LL + ty;
+        }
     }
 
     // --- CSR (bit-exact with the reference) and its node-block view
@@ -410,6 +434,11 @@ extern "C" void sw2g_destroy(sw2g_model* m) {
     for (void* p : m->allocs) cudaFree(p);
     if (m->h_rout) cudaFreeHost(m->h_rout);
     if (m->h_ks) cudaFreeHost(m->h_ks);
+    if (m->h_pflag) cudaFreeHost(m->h_pflag);
+    if (m->h_cptr) cudaFreeHost(m->h_cptr);
+    if (m->h_cown) cudaFreeHost(m->h_cown);
+    if (m->h_cnode) cudaFreeHost(m->h_cnode);
+    if (m->h_crofs) cudaFreeHost(m->h_crofs);
     for (auto& r : m->prof_pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : m->ev_pool) cudaEventDestroy(e);
     if (m->own_stream) cudaStreamDestroy(m->st);
@@ -488,13 +517,21 @@ static int do_prepare(sw2g_model* m, double* vals, double* res, double* x) {
 }
 static int build_amg(sw2g_model* m);
 // preconditioner set-up on the scaled matrix (replaces prep_umfpack, bcgstab_solver.c:371)
-static int do_precond_setup(sw2g_model* m, const double* vals, int precond) {
+static int build_patches(sw2g_model* m, const double* vals);
+static void invalidate_graphs(sw2g_model* m);
+static int do_precond_setup(sw2g_model* m, const double* vals, int precond, int chunks = 0) {
     if (precond == SW2G_PC_AMG) {
         if (!m->amg_ready) TRY(build_amg(m));
-        ProfScope ps(m, 3, 1 + 4 * (m->amg.nlev - 1));
-        amg_setup(m->B, m->amg, m->A, vals, m->st);
-        CKL();
-        return SW2G_OK;
+        if (m->amg.patch.mode != chunks) {   // the placement is baked into the captured solver graphs
+            invalidate_graphs(m);
+            m->amg.patch.mode = chunks;
+        }
+        {
+            ProfScope ps(m, 3, 1 + 4 * (m->amg.nlev - 1));
+            amg_setup(m->B, m->amg, m->A, vals, m->st);
+            CKL();
+        }
+        return build_patches(m, vals);
     }
     if (precond == SW2G_PC_BILU0) {
         ProfScope ps(m, 3, 1 + m->ilu.ncolors);
@@ -622,6 +659,18 @@ static int build_amg(sw2g_model* m) {
         TRY(up(&D.gptr, K[l].gptr)); TRY(up(&D.gsrc, K[l].gsrc));
     }
     TRY(dalloc(m, &A.dinv0_64, 9 * (size_t)m->V)); TRY(dalloc(m, &A.dinv0_32, 9 * (size_t)m->V));
+    {   // chunk corrections: flags and counters now, the chunk buffers on the first build
+        PatchDev& P = A.patch;
+        TRY(dalloc(m, &P.flag, (size_t)m->V)); TRY(dalloc(m, &P.counts, 2)); TRY(dalloc(m, &P.failed, 1));
+        CK(cudaMemsetAsync(P.counts, 0, 2 * sizeof(int), m->st));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+        P.grid = 4 * (sms > 0 ? sms : 148);
+        P.mode = 0;   // set per solve from sw2g_newton_opts.amg_chunks
+        if (cudaMallocHost((void**)&m->h_pflag, sizeof(int) * (size_t)m->V) != cudaSuccess) {
+            g_err = "cudaMallocHost failed"; return SW2G_ERR_NOMEM;
+        }
+    }
     m->amg_ready = true;
     static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;
     if (trace) {
@@ -632,10 +681,133 @@ static int build_amg(sw2g_model* m) {
     return SW2G_OK;
 }
 
+// Drops every captured solver graph (their kernels hold buffer addresses that are about to change).
+static void invalidate_graphs(sw2g_model* m) {
+    cudaStreamSynchronize(m->st);
+    for (int k = 0; k < 3; k++) {
+        if (m->graph64[k]) { cudaGraphExecDestroy(m->graph64[k]); m->graph64[k] = nullptr; }
+        if (m->graph32[k]) { cudaGraphExecDestroy(m->graph32[k]); m->graph32[k] = nullptr; }
+    }
+    if (m->gm_graph64) { cudaGraphExecDestroy(m->gm_graph64); m->gm_graph64 = nullptr; }
+    if (m->gm_graph32) { cudaGraphExecDestroy(m->gm_graph32); m->gm_graph32 = nullptr; }
+    if (m->gm_graph_b32) { cudaGraphExecDestroy(m->gm_graph_b32); m->gm_graph_b32 = nullptr; }
+    m->gm_m64 = m->gm_m32 = m->gm_mb32 = -1;
+}
+
+// Chunks of the flagged nodes for the AMG's level-0 corrections (amg_kernels.cu).  The
+// patch set is every node whose smoother block the l1 fix-up weakened (flags written by
+// amg_setup) plus its neighbours.  Its nodes are taken tile by tile (tiles of
+// kPatchTileEdges mean edge lengths), in node order within a tile; a chunk owns a run of
+// them and extends over their neighbours in the patch set, closed before it would pass
+// kPatchMaxNodes nodes.  Own nodes are listed first.  Deterministic: the same flags give
+// the same chunks.  The chunk blocks are then inverted on the device.
+static int build_patches(sw2g_model* m, const double* vals) {
+    PatchDev& P = m->amg.patch;
+    const int V = m->V;
+    if (P.mode == 0) return SW2G_OK;
+    ProfScope ps(m, 3, 1);
+    CK(cudaMemcpyAsync(m->h_pflag, P.flag, sizeof(int) * (size_t)V, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    const std::vector<int>& bp = m->h_bptr;
+    const std::vector<int>& bc = m->h_bcol;
+    std::vector<char> inp(V, 0);
+    int nflag = 0;
+    for (int i = 0; i < V; i++)
+        if (m->h_pflag[i]) {
+            nflag++;
+            for (int q = bp[i]; q < bp[i + 1]; q++) inp[bc[q]] = 1;
+        }
+    std::vector<std::pair<long long, int>> pn;
+    for (int i = 0; i < V; i++) if (inp[i]) pn.emplace_back(m->h_tile[i], i);
+    std::sort(pn.begin(), pn.end());
+    std::vector<int> cptr(1, 0), cown, cnode;
+    std::vector<long long> crofs;
+    std::vector<int> stamp(V, -1);
+    std::vector<char> role(V, 0);   // 1 own, 0 ring
+    std::vector<int> own, members;
+    long long rtot = 0;
+    int piece = 0;
+    auto finalize = [&]() {
+        if (own.empty()) return;
+        for (int a : own) cnode.push_back(a);
+        for (int a : members) if (!role[a]) cnode.push_back(a);
+        const int ne = (int)cnode.size() - cptr.back();
+        crofs.push_back(rtot);
+        rtot += 9LL * (long long)own.size() * ne;
+        cown.push_back((int)own.size());
+        cptr.push_back((int)cnode.size());
+        own.clear(); members.clear();
+        piece++;
+    };
+    for (size_t k = 0; k < pn.size(); k++) {
+        if (k > 0 && pn[k].first != pn[k - 1].first) finalize();
+        const int a = pn[k].second;
+        int add = (stamp[a] != piece) ? 1 : 0;
+        for (int q = bp[a]; q < bp[a + 1]; q++) { const int b = bc[q]; if (inp[b] && stamp[b] != piece && b != a) add++; }
+        if ((int)members.size() + add > kPatchMaxNodes) finalize();
+        if (stamp[a] != piece) { stamp[a] = piece; members.push_back(a); }
+        role[a] = 1;
+        own.push_back(a);
+        for (int q = bp[a]; q < bp[a + 1]; q++) {
+            const int b = bc[q];
+            if (inp[b] && stamp[b] != piece) { stamp[b] = piece; role[b] = 0; members.push_back(b); }
+        }
+    }
+    finalize();
+    const int nch = (int)cown.size(), nent = (int)cnode.size();
+    // capacities (grown with headroom; growing changes addresses the captured graphs hold)
+    if (m->pcap_chunks == 0 || nch > m->pcap_chunks || nent > m->pcap_entries || rtot > m->pcap_r) {
+        invalidate_graphs(m);
+        const int cc = std::max(m->pcap_chunks, nch + nch / 4 + 64);
+        const int ce = std::max(m->pcap_entries, nent + nent / 4 + 256);
+        const long long cr = std::max(m->pcap_r, rtot + rtot / 4 + 4096);
+        dfree(m, &P.chunk_ptr); dfree(m, &P.own_cnt); dfree(m, &P.rofs); dfree(m, &P.ext_node);
+        dfree(m, &P.r64); dfree(m, &P.r32); dfree(m, &P.e64); dfree(m, &P.e32);
+        TRY(dalloc(m, &P.chunk_ptr, (size_t)cc + 1)); TRY(dalloc(m, &P.own_cnt, (size_t)cc));
+        TRY(dalloc(m, &P.rofs, (size_t)cc)); TRY(dalloc(m, &P.ext_node, (size_t)ce));
+        TRY(dalloc(m, &P.r64, (size_t)cr)); TRY(dalloc(m, &P.r32, (size_t)cr));
+        TRY(dalloc(m, &P.e64, 3 * (size_t)ce)); TRY(dalloc(m, &P.e32, 3 * (size_t)ce));
+        if (m->h_cptr) { cudaFreeHost(m->h_cptr); cudaFreeHost(m->h_cown); cudaFreeHost(m->h_cnode); cudaFreeHost(m->h_crofs); }
+        if (cudaMallocHost((void**)&m->h_cptr, sizeof(int) * ((size_t)cc + 3)) != cudaSuccess ||
+            cudaMallocHost((void**)&m->h_cown, sizeof(int) * (size_t)cc) != cudaSuccess ||
+            cudaMallocHost((void**)&m->h_cnode, sizeof(int) * (size_t)ce) != cudaSuccess ||
+            cudaMallocHost((void**)&m->h_crofs, sizeof(long long) * (size_t)cc) != cudaSuccess) {
+            g_err = "cudaMallocHost failed"; return SW2G_ERR_NOMEM;
+        }
+        m->pcap_chunks = cc; m->pcap_entries = ce; m->pcap_r = cr;
+    }
+    // staging: chunk_ptr [nch+1], then the two counts in the slots after it
+    std::copy(cptr.begin(), cptr.end(), m->h_cptr);
+    std::copy(cown.begin(), cown.end(), m->h_cown);
+    std::copy(cnode.begin(), cnode.end(), m->h_cnode);
+    std::copy(crofs.begin(), crofs.end(), m->h_crofs);
+    m->h_cptr[nch + 1] = nch; m->h_cptr[nch + 2] = nent;
+    CK(cudaMemcpyAsync(P.chunk_ptr, m->h_cptr, sizeof(int) * ((size_t)nch + 1), cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(P.counts, m->h_cptr + nch + 1, 2 * sizeof(int), cudaMemcpyHostToDevice, m->st));
+    if (nch > 0) {
+        CK(cudaMemcpyAsync(P.own_cnt, m->h_cown, sizeof(int) * (size_t)nch, cudaMemcpyHostToDevice, m->st));
+        CK(cudaMemcpyAsync(P.rofs, m->h_crofs, sizeof(long long) * (size_t)nch, cudaMemcpyHostToDevice, m->st));
+        CK(cudaMemcpyAsync(P.ext_node, m->h_cnode, sizeof(int) * (size_t)nent, cudaMemcpyHostToDevice, m->st));
+    }
+    CK(cudaMemsetAsync(P.failed, 0, sizeof(int), m->st));
+    patch_invert(m->B, P, vals, nch, m->st);
+    CKL();
+    m->p_nchunks = nch; m->p_nentries = nent; m->p_nflag = nflag; m->p_rtot = rtot;
+    static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;
+    if (trace) {
+        int failed = 0;
+        CK(cudaMemcpyAsync(&failed, P.failed, sizeof(int), cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        fprintf(stderr, "amg chunks: %d flagged nodes, %zu patch nodes, %d chunks, %d entries, %lld inverse entries, %d singular\n",
+                nflag, pn.size(), nch, nent, rtot, failed);
+    }
+    return SW2G_OK;
+}
+
 // kernel launches of one preconditioner application (profiling counts)
 static int precond_launches(const sw2g_model* m, int precond) {
     if (precond == SW2G_PC_BILU0) return 2 * m->ilu.ncolors;
-    if (precond == SW2G_PC_AMG) return 1 + (m->amg.nlev - 1) * (2 * kAmgNu + 4) + 1;
+    if (precond == SW2G_PC_AMG) return 1 + (m->amg.nlev - 1) * (2 * kAmgNu + 4) + 1 + 2;
     return 1;
 }
 
@@ -900,7 +1072,7 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
     const double target = std::max(o.krylov_tol * fnorm, (o.tol_nonlin_rel > 0.0 ? 0.1 : 0.01) * o.tol_nonlin);
     *iters = 0; *passes = 0; *status = 0;
     double prev = 0;
-    int stall = 0;
+    int stall = 0, slow = 0;
     int hstate[4] = {0, 0, 0, 0};
     double hscal[3] = {0, 0, 0};
     static const bool trace = getenv("SW2G_TRACE_KRYLOV") != nullptr;   // diagnostic: pass history on stderr
@@ -927,8 +1099,10 @@ static int solve_gmres(sw2g_model* m, double* x, double* b, const sw2g_newton_op
         if (!std::isfinite(rn)) { *status = 2; break; }
         if (!(rn > target)) break;
         if (pass > 0) {
+            // stalled: three passes in a row gaining less than 1%, or five gaining less than 10%
             stall = (rn > 0.99 * prev) ? stall + 1 : 0;
-            if (stall >= 3) {
+            slow = (rn > 0.9 * prev) ? slow + 1 : 0;
+            if (stall >= 3 || slow >= 5) {
                 *status = 4;
                 if (trace) {   // where the stalled linear residual sits (largest unscaled entries)
                     std::vector<double> t(n), sc(n);
@@ -1091,7 +1265,8 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
     if (!(valid_precond(o_in.precond) && (o_in.krylov_precision == 32 || o_in.krylov_precision == 64) && o_in.krylov_max_it >= 0 &&
           (o_in.krylov_method == SW2G_KRYLOV_BICGSTAB ||
            (o_in.krylov_method == SW2G_KRYLOV_GMRES && o_in.precond != SW2G_PC_BLOCK_JACOBI)) &&
-          o_in.max_nonlin_it >= 0 && o_in.max_linesearch_cuts >= 0 && o_in.max_refine >= 0)) {
+          o_in.max_nonlin_it >= 0 && o_in.max_linesearch_cuts >= 0 && o_in.max_refine >= 0 &&
+          o_in.amg_chunks >= 0 && o_in.amg_chunks <= 2)) {
         g_err = "sw2g newton: bad options";
         return SW2G_ERR_ARG;
     }
@@ -1153,12 +1328,13 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
     sw2g_newton_opts o = o_in;   // the step's effective options
     // relative test: against the previous-step state's residual, the same reference with or without a guess
     if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = o_in.tol_nonlin_rel * st.prev_resid_max;
-    int it = 0; bool ok = true, keep, lin_ok = true;
+    int it = 0, stalled_its = 0; bool ok = true, keep, lin_ok = true;
+    double rmax_prev = rmax;
     do {
         TRY(do_jacobian(m, m->d_sol, m->d_sol_old, m->d_sol_older, m->d_vals));
         CK(cudaMemsetAsync(m->d_dsol, 0, sizeof(double) * n, m->st));
         TRY(do_prepare(m, m->d_vals, m->d_res, m->d_dsol));
-        TRY(do_precond_setup(m, m->d_vals, o.precond));
+        TRY(do_precond_setup(m, m->d_vals, o.precond, o.amg_chunks));
         int kit = 0, kst = 0, passes = 0;
         if (o.krylov_method == SW2G_KRYLOV_GMRES)
             TRY(solve_gmres(m, m->d_dsol, m->d_res, o, o.krylov_precision == 32, rmax, &kit, &passes, &kst));
@@ -1202,13 +1378,18 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
         // with an iterative solve that stopped early it may only mean the solve stalled.
         lin_ok = (lin_status == 0);
         if (!lin_ok) st.linear_unconverged++;
+        // a stalled linear solve that does not halve max|R| twice in a row ends the solve as failed:
+        // retrying the interval with a smaller dt is cheaper than the remaining stalled iterations
+        stalled_its = (lin_status == 4 && !(rmax < 0.5 * rmax_prev)) ? stalled_its + 1 : 0;
+        rmax_prev = rmax;
         st.linesearch_cuts += cuts;
         it++;
         static const bool trace = getenv("SW2G_TRACE_NEWTON") != nullptr;   // diagnostic: Newton history on stderr
         if (trace)
             fprintf(stderr, "newton it %d krylov %d status %d refine %d resid_max %.3e resid_l2 %.3e inc_max %.3e cuts %d\n",
                     it, kit, kst, passes, rmax, rl2, imax, cuts);
-        keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && (imax > o.inc_nonlin || !lin_ok);
+        keep = ok && it < o.max_nonlin_it && rmax < 1.0E+20 && rmax > o.tol_nonlin && (imax > o.inc_nonlin || !lin_ok) &&
+               stalled_its < 2;
     } while (keep);
     st.newton_its = it;
     st.resid_max = rmax; st.resid_l2 = rl2; st.inc_max = imax;
@@ -1495,6 +1676,17 @@ extern "C" int sw2g_grid_mass(sw2g_model* m, const double* sol, double density, 
     return SW2G_OK;
 }
 
+extern "C" int sw2g_precond_info(sw2g_model* m, long long* info) {
+    NEED(m && info, "sw2g_precond_info: null argument");
+    int failed = 0;
+    if (m->amg.patch.failed) {
+        CK(cudaMemcpyAsync(&failed, m->amg.patch.failed, sizeof(int), cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+    }
+    info[0] = m->p_nflag; info[1] = m->p_nchunks; info[2] = m->p_nentries; info[3] = m->p_rtot; info[4] = failed;
+    return SW2G_OK;
+}
+
 extern "C" int sw2g_set_profiling(sw2g_model* m, int on) {
     NEED(m, "null model");
     m->prof = on != 0;
@@ -1514,16 +1706,18 @@ extern "C" int sw2g_reset_profile(sw2g_model* m) {
 }
 
 extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_ms, double* bytes) {
-    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 6, "sw2g_time_kernel: bad argument");
+    NEED(m && avg_ms && bytes && reps > 0 && which >= 0 && which <= 9, "sw2g_time_kernel: bad argument");
+    NEED(which != 8 || m->gm_graph_b32, "sw2g_time_kernel: no FP32 GMRES cycle has run yet");
     const double nnz = m->nnz, n = m->n, T = m->T, S = m->S;
     if (which >= 4) {   // the AMG sweeps
         if (!m->amg_ready) TRY(build_amg(m));
         amg_setup(m->B, m->amg, m->A, m->d_vals, m->st);
     }
-    if (which == 5 || which == 6) {
+    if (which == 5 || which == 6 || which == 7 || which == 9) {
         TRY(alloc_fp32(m));
         launch_to_float(m->nnz, m->d_vals, m->f_vals, m->st);
     }
+    const double zero = 0.0;
     auto launch = [&]() {
         switch (which) {
             case 0: launch_spmv64(m->B, m->d_vals, m->k_p, m->k_Ap, m->st); break;
@@ -1533,6 +1727,12 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
             case 4: amg_smooth0_once(m->B, m->amg, m->d_vals, m->k_p, m->k_Ap, m->k_As, m->st); break;
             case 5: amg_smooth0_once32(m->B, m->amg, m->f_vals, m->f_p, m->f_Ap, m->f_As, m->st); break;
             case 6: amg_apply<float>(m->B, m->amg, m->f_vals, m->f_Ap, nullptr, m->st); break;
+            case 7: spmv_skip<float>(m->B, m->f_vals, m->f_p, m->f_Ap, nullptr, m->st); break;
+            case 8:   // a whole FP32 GMRES cycle with its stopping test off: every iteration runs
+                cudaMemcpyAsync(m->gm.scal + 3, &zero, sizeof(double), cudaMemcpyHostToDevice, m->st);
+                cudaGraphLaunch(m->gm_graph_b32, m->st);
+                break;
+            case 9: amg_patch_correct<float>(m->B, m->amg, m->f_vals, m->f_p, m->f_Ap, nullptr, m->st); break;
 
         }
     };
@@ -1556,6 +1756,9 @@ extern "C" int sw2g_time_kernel(sw2g_model* m, int which, int reps, double* avg_
         case 4: *bytes = 12.0 * nnz + 20.0 * n + 24.0 * n + 16.0 * n; break;    // SpMV + block-Jacobi apply
         case 6: *bytes = 4.0 * (8.0 * nnz + 32.0 * n); break;   // ~4 level-0 matrix passes (coarse levels extra)
         case 5: *bytes = 8.0 * nnz + 12.0 * n + 12.0 * n + 8.0 * n; break;   // FP32 SpMV + FP32 block apply
+        case 7: *bytes = 8.0 * nnz + 12.0 * n; break;                        // FP32 values + cols, x and y
+        case 8: *bytes = (double)m->gm_mb32; break;                          // iterations of the cycle (not bytes)
+        case 9: *bytes = 4.0 * (double)m->p_rtot + 12.0 * m->p_nentries; break;   // FP32 inverse rows + residuals
     }
     return SW2G_OK;
 }

@@ -127,11 +127,34 @@ struct AmgLink {                        // level l -> level l+1
     const int* gptr = nullptr;          // [nb_{l+1}+1] fine blocks summed into each coarse block
     const int* gsrc = nullptr;          // level 0: slot ids of the node graph; else block ids
 };
+// Chunked exact solves on the level-0 nodes where the l1 fix-up leaves block-Jacobi
+// smoothing nearly inert (shallow nodes along the wet/dry front): the flagged nodes and
+// their neighbours are cut into chunks of at most kPatchMaxNodes nodes (own nodes plus one
+// ring of overlap), each chunk's dense block of the scaled matrix is inverted once per
+// Newton iteration, and after every level-0 V-cycle each chunk corrects its own nodes
+// with its rows of that inverse (restricted additive Schwarz).
+constexpr int kPatchMaxNodes = 53;          // 159 dofs: the dense chunk matrix fits in shared memory
+constexpr double kPatchFlagRatio = 0.5;     // flag: sum |l1 block inverse| < ratio * sum |plain block inverse|
+struct PatchDev {                           // device pointers (capacities kept by the host driver)
+    int* flag = nullptr;                    // [nnodes] written by the level-0 smoother set-up
+    int* counts = nullptr;                  // [2] chunks, ext entries of the current build
+    int* chunk_ptr = nullptr;               // [chunks+1] offsets into ext_node
+    int* own_cnt = nullptr;                 // [chunks] own nodes (listed first in the chunk's ext nodes)
+    long long* rofs = nullptr;              // [chunks] offset of the chunk's inverse rows
+    int* ext_node = nullptr;                // [entries] chunk nodes, own first then the ring
+    double* r64 = nullptr; float* r32 = nullptr;   // own-dof rows of each chunk inverse, row-major
+    double* e64 = nullptr; float* e32 = nullptr;   // [3*entries] residual at the chunk nodes
+    int* failed = nullptr;                  // [1] chunks whose inversion met a zero pivot (left uncorrected)
+    int grid = 0;                           // CTAs of the correction kernels (grid-stride over chunks)
+    int mode = 0;                           // 0 off, 1 after each V-cycle, 2 inside it (after the level-0
+                                            // pre-smoothing and after the post-smoothing)
+};
 struct AmgHost {
     int nlev = 0;                       // levels including level 0
     AmgLevel lev[kAmgMaxLevels];
     AmgLink link[kAmgMaxLevels];
     double* dinv0_64 = nullptr; float* dinv0_32 = nullptr;   // [9*nnodes] level-0 smoother blocks
+    PatchDev patch;                     // level-0 chunk corrections (inactive while patch.flag is null)
 };
 template <class VT> struct AmgBuf;
 template <> struct AmgBuf<double> {
@@ -152,16 +175,22 @@ template <> struct AmgBuf<float> {
     static float* t(const AmgLevel& L) { return L.t32; }
     static float* r(const AmgLevel& L) { return L.r32; }
 };
-// numeric set-up from the scaled level-0 matrix (FP64, plus FP32 copies)
+// numeric set-up from the scaled level-0 matrix (FP64, plus FP32 copies); writes H.patch.flag
 void amg_setup(const BlockCSR& A, const AmgHost& H, const AssemblyMaps& maps, const double* vals, cudaStream_t st);
+// inverts the chunk blocks of the current patch build (nchunks from the host build)
+void patch_invert(const BlockCSR& A, const PatchDev& P, const double* vals, int nchunks, cudaStream_t st);
 // one level-0 smoothing sweep y = x + w Dinv (b - A x) (FP64; kernel timing)
 void amg_smooth0_once(const BlockCSR& A, const AmgHost& H, const double* vals, const double* b, const double* x, double* y,
                       cudaStream_t st);
 void amg_smooth0_once32(const BlockCSR& A, const AmgHost& H, const float* vals, const float* b, const float* x, float* y,
                         cudaStream_t st);
-// y <- V-cycle(y); vals0 = the level-0 values in the Krylov precision
+// y <- V-cycle(y) followed by the chunk corrections; vals0 = the level-0 values in the Krylov precision
 template <class VT>
 void amg_apply(const BlockCSR& A, const AmgHost& H, const VT* vals0, VT* y, const int* skip, cudaStream_t st);
+// y += the chunk corrections of the residual b - A y (the last stage of amg_apply)
+template <class VT>
+void amg_patch_correct(const BlockCSR& A, const AmgHost& H, const VT* vals0, const VT* b, VT* y, const int* skip,
+                       cudaStream_t st);
 
 // ---- preconditioner dispatch for the BiCGStab "_pc" path
 template <class VT>

@@ -288,6 +288,20 @@ def run_ours(args, world, rank, local, dist):
     rf_ms, rf_bytes = fast.model.time_kernel(5, 20)
     spmv_ms, spmv_bytes = fast.model.time_kernel(0, 20)
     fd_ms, fd_bytes = fast.model.time_kernel(1, 5)
+    # one FP32 GMRES iteration of the fast path, by part (CUDA events on the model's stream)
+    breakdown = None
+    try:
+        cyc_ms, cyc_its = fast.model.time_kernel(8, 3)
+        vc_ms, _ = fast.model.time_kernel(6, 10)
+        sp32_ms, _ = fast.model.time_kernel(7, 20)
+        pc_ms, pc_bytes = fast.model.time_kernel(9, 20)
+        it_ms = cyc_ms / max(cyc_its, 1.0)
+        breakdown = {"iteration_ms": it_ms, "amg_vcycle_ms": vc_ms, "of_which_level0_sweeps_ms": 4 * rf_ms,
+                     "of_which_chunk_correction_ms": pc_ms, "spmv_ms": sp32_ms,
+                     "gram_schmidt_and_vector_ops_ms": it_ms - vc_ms - sp32_ms, "cycle_iterations": cyc_its,
+                     "chunk_correction_bytes": pc_bytes}
+    except Exception as e:  # noqa: BLE001 - reported, not fatal
+        breakdown = {"error": str(e)}
     peaks = {}
     try:
         with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as fh:
@@ -429,7 +443,8 @@ def run_ours(args, world, rank, local, dist):
                      "avg_launch_ms": rf_ms,
                      "spmv_fp64": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "avg_launch_ms": spmv_ms,
                                    "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / hbm},
-                     "fd_jacobian": {"achieved_gbs": fd_bytes / (fd_ms * 1e-3) / 1e9, "avg_launch_ms": fd_ms}},
+                     "fd_jacobian": {"achieved_gbs": fd_bytes / (fd_ms * 1e-3) / 1e9, "avg_launch_ms": fd_ms},
+                     "gmres_iteration_fp32": breakdown},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "error_vs_reference_sample": sample_err,

@@ -68,6 +68,11 @@ typedef struct {
                                  and the Gram-Schmidt in FP64 around the FP32 preconditioner; 32 runs the whole
                                  cycle in FP32, each cycle refined from the FP64 residual */
     int krylov_restart;       /* GMRES restart length, 1..200 (default 30); the basis holds restart+1 vectors */
+    int amg_chunks;           /* AMG chunk corrections (exact solves on chunks of the nodes whose block-Jacobi
+                                 smoothing the l1 fix-up weakens): 0 off (default), 1 after each V-cycle,
+                                 2 inside it.  They remove the stall of the linear solve at shallow wet/dry
+                                 nodes on some steps and slow or break it on others (nearly singular chunk
+                                 blocks), so they are off unless asked for. */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's
@@ -220,6 +225,12 @@ int sw2g_device_state(sw2g_model *m, double **sol, double **sol_old, double **so
 void *sw2g_stream(sw2g_model *m);
 
 /* --- instrumentation ------------------------------------------------------ */
+/* The AMG's chunk corrections at the last preconditioner set-up: info[0] nodes whose
+ * smoother block the l1 fix-up weakened, info[1] chunks, info[2] chunk nodes (with
+ * overlap), info[3] entries of the inverse rows kept, info[4] chunks left uncorrected
+ * because their block was singular.  No counterpart in the reference (its UMFPACK LU
+ * needs no such correction). */
+int sw2g_precond_info(sw2g_model *m, long long *info);
 /* Per kernel class, CUDA-event time (ms) and launch counts since the last reset:
  * classes 0 residual, 1 FD Jacobian, 2 Jacobian gather, 3 Dirichlet/scale/precond
  * setup, 4 BiCGStab, 5 other.  Timing adds events around each class. */
@@ -231,7 +242,10 @@ int sw2g_reset_profile(sw2g_model *m);
  * model's stream) and returns the mean launch time and the algorithmic bytes of
  * one launch: 0 FP64 SpMV, 1 FD Jacobian element kernels, 2 element residual,
  * 3 Jacobian gather, 4 AMG level-0 smoothing sweep (FP64), 5 the same sweep on FP32
- * values and vectors, 6 one FP32 AMG V-cycle (bytes: its four level-0 matrix passes).
+ * values and vectors, 6 one FP32 AMG V-cycle (bytes: its four level-0 matrix passes),
+ * 7 FP32 SpMV, 8 one whole FP32 GMRES cycle with its stopping test off (bytes: the
+ * cycle's iteration count, so avg_ms / bytes is one iteration; needs a prior FP32 GMRES
+ * solve), 9 the AMG's chunk corrections in FP32 (bytes: inverse rows and residuals read).
  * Instrumentation for roofline
  * reporting; no counterpart in the reference. */
 int sw2g_time_kernel(sw2g_model *m, int which, int reps, double *avg_ms, double *bytes);
