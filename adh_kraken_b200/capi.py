@@ -43,7 +43,7 @@ class NewtonOpts(C.Structure):
                 ("krylov_precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
                 ("use_guess", C.c_int), ("precond", C.c_int), ("krylov_method", C.c_int),
                 ("tol_nonlin_rel", C.c_double), ("krylov_basis_precision", C.c_int), ("krylov_restart", C.c_int),
-                ("amg_chunks", C.c_int)]
+                ("amg_chunks", C.c_int), ("tol_nonlin_min", C.c_double)]
 
 PC_BLOCK_JACOBI = 0
 PC_BILU0 = 1

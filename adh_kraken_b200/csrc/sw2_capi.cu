@@ -204,6 +204,7 @@ extern "C" void sw2g_default_opts(sw2g_newton_opts* o) {
     o->krylov_basis_precision = 64;
     o->krylov_restart = 30;
     o->amg_chunks = 0;
+    o->tol_nonlin_min = 0.0;
 }
 
 extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model** out) {
@@ -1327,7 +1328,7 @@ static int newton_device(sw2g_model* m, const sw2g_newton_opts& o_in, sw2g_newto
     st.initial_resid_l2 = rl2;
     sw2g_newton_opts o = o_in;   // the step's effective options
     // relative test: against the previous-step state's residual, the same reference with or without a guess
-    if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = o_in.tol_nonlin_rel * st.prev_resid_max;
+    if (o_in.tol_nonlin_rel > 0.0) o.tol_nonlin = std::max(o_in.tol_nonlin_rel * st.prev_resid_max, o_in.tol_nonlin_min);
     int it = 0, stalled_its = 0; bool ok = true, keep, lin_ok = true;
     double rmax_prev = rmax;
     do {

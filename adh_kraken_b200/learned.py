@@ -292,13 +292,15 @@ def generate_trajectory(case, nsteps, opts=None, spinup=0, with_masks=False):
     return states[spinup:]
 
 
-def set_normalisation(net, trajs):
+def set_normalisation(net, trajs, stride=1):
+    """Feature means / deviations and the correction scale from the trajectories (every
+    ``stride``-th snapshot, to bound the host memory on long runs)."""
     import torch
     feats, corr = [], []
     for tr in trajs:
-        S = tr.S.cpu().numpy()
         z = tr.z.cpu().numpy()
-        for t in range(1, len(S) - 1):
+        for t in range(1, len(tr) - 1, stride):
+            S = {k: tr.S[k].cpu().numpy() for k in (t - 1, t, t + 1)}
             s, p, nx = S[t].reshape(-1, 3), S[t - 1].reshape(-1, 3), S[t + 1].reshape(-1, 3)
             f = np.concatenate([s, s - p, z[:, None], (s[:, :1] > 0).astype(np.float64)], axis=1)
             feats.append(f)
@@ -437,3 +439,110 @@ def main(out=WEIGHTS, nsteps=12, seed=4, iters=300, nx=2828, ny=707, krylov_tol=
 
 if __name__ == "__main__":
     main()
+
+
+def device_trajectory(case, nsteps, opts=None):
+    """Like generate_trajectory, but each state goes to a device tensor as soon as it is
+    read back, so long runs on large meshes need no host memory for the set."""
+    import torch
+    from .capi import SW2Error
+    from .timeloop import SW2Simulation
+    sim = SW2Simulation(case, opts=opts)
+    S = [torch.tensor(sim.state()[0], device="cuda")]
+    for _ in range(nsteps):
+        try:
+            st = sim.step()
+        except SW2Error as e:
+            print(f"trajectory stops: {e}", flush=True)
+            break
+        if not st["success"]:
+            print(f"trajectory stops: step not converged", flush=True)
+            break
+        S.append(torch.tensor(sim.state()[0], device="cuda"))
+    sim.model.close()
+    tr = Trajectory.__new__(Trajectory)
+    tr.S = torch.stack(S)
+    tr.z = torch.tensor(case.xyz[:, 2].astype(np.float64), device="cuda")
+    return tr
+
+
+def evaluate_guess(net, case, nsteps, opts):
+    """Runs ``nsteps`` steps of ``case`` twice from its initial state: Newton started from
+    the previous step (the reference's start) and from the network's guess (use_guess = 1;
+    the residual still judges it).  Per run: Newton and Krylov iterations, steps the guess
+    started, and device time (CUDA events on the model's stream, guess inference
+    included)."""
+    import copy
+    import torch
+    from .timeloop import SW2Simulation
+    out = {}
+    for mode in ("previous_step", "learned"):
+        o = copy.copy(opts)
+        o.use_guess = 1 if mode == "learned" else 0
+        sim = SW2Simulation(case, opts=o)
+        g = Guesser(net, case) if mode == "learned" else None
+        s = torch.cuda.ExternalStream(sim.model.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        rec = {"newton_its": 0, "krylov_its": 0, "guess_used": 0, "failed": 0, "steps": 0}
+        torch.cuda.synchronize()
+        ev0.record(s)
+        for _ in range(nsteps):
+            if g is not None and len(sim.history) > 0:    # the guess needs two states
+                g.predict_into(sim)
+            st = sim.step()
+            rec["newton_its"] += st["newton_its"]; rec["krylov_its"] += st["krylov_its"]
+            rec["guess_used"] += st.get("guess_used", 0); rec["failed"] += int(not st["success"])
+            rec["steps"] += 1
+        ev1.record(s)
+        torch.cuda.synchronize()
+        rec["ms"] = ev0.elapsed_time(ev1)
+        rec["steps_per_s"] = rec["steps"] / (rec["ms"] * 1e-3)
+        rec["final_state"] = sim.state()[0]
+        sim.model.close()
+        out[mode] = rec
+    a, b = out["previous_step"]["final_state"], out["learned"]["final_state"]
+    out["state_rel_diff"] = [float(np.abs(a[k::3] - b[k::3]).max() / max(np.abs(a[k::3]).max(), 1e-300))
+                             for k in range(3)]
+    for mode in ("previous_step", "learned"):
+        del out[mode]["final_state"]
+    return out
+
+
+def config4(n=707, train_seeds=tuple(range(40, 48)), test_seeds=tuple(range(48, 52)), steps_per_traj=375,
+            eval_steps=40, iters=2000, out=None, opts=None, log=print):
+    """The learned-guess experiment on the basin with inflow hydrographs
+    (mesh.basin_hydro_case): trajectories of the solver under the training hydrographs
+    (8 x 375 = 3000 steps at the default sizes), the network trained on them by the
+    library's kernels, then Newton / Krylov work and device time on the held-out
+    hydrographs with and without the learned guess."""
+    import time
+    from .capi import default_opts
+    from .mesh import basin_hydro_case
+    opts = opts or default_opts(precond=2, krylov_method=1, krylov_precision=32, krylov_basis_precision=32,
+                                krylov_tol=1e-6, tol_nonlin_rel=1e-8, krylov_max_it=20000, krylov_restart=50)
+    t0 = time.time()
+    trajs = []
+    for sd in train_seeds:
+        case = basin_hydro_case(sd, n=n, nsteps=steps_per_traj + 2)
+        trajs.append(device_trajectory(case, steps_per_traj, opts))
+        log(f"trajectory {sd}: {len(trajs[-1])} states, {time.time() - t0:.0f} s")
+    graph = DeviceGraph(build_graph(case.xyz[:, :2], case.tri))
+    net = Net()
+    set_normalisation(net, trajs, stride=max(1, steps_per_traj // 25))
+    before = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
+    losses = train(net, graph, trajs, iters=iters, log_every=max(1, iters // 10))
+    after = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
+    log(f"trained {iters} iterations: loss {before:.4f} (linear extrapolation) -> {after:.4f}, {time.time() - t0:.0f} s")
+    del trajs
+    res = {"train_states": sum(1 for _ in train_seeds) * steps_per_traj, "loss_before": before, "loss_after": after,
+           "losses": losses, "held_out": {}}
+    for sd in test_seeds:
+        case = basin_hydro_case(sd, n=n, nsteps=eval_steps + 2)
+        res["held_out"][sd] = evaluate_guess(net, case, eval_steps, opts)
+        res["held_out"][sd]["q_peak"] = case.q_peak
+        log(f"held-out {sd}: {res['held_out'][sd]}")
+    if out:
+        net.save(out, meta={"workload": "basin_hydro", "n": n, "train_seeds": list(train_seeds),
+                            "steps_per_traj": steps_per_traj, "iters": iters, "loss_before": before,
+                            "loss_after": after})
+    return net, res

@@ -281,3 +281,26 @@ def small_delaunay_case(n: int = 24, seed: int = 7, wetdry: bool = True, nsteps:
     series = {0: (np.array([0.0, tf]), np.array([2.1, 2.2])), 1: (np.array([0.0, tf]), np.array([0.05, 0.08])),
               2: _const_series(0.0, tf, 0.01)}
     return SW2Case("delaunay_small", xyz, tri, seg, kind, sol0, dt, nsteps, series)
+
+
+def basin_hydro_case(hydro_seed: int, n: int = 707, seed: int = 2, nsteps: int = 375, dt: float = 300.0) -> SW2Case:
+    """The learned-guess workload: the fully wet tidal basin of :func:`basin_case` (same
+    mesh, bathymetry and 1 m / 12.42 h tide on the west edge) with an inflow hydrograph on
+    the east edge, Q(t) = 200 + (Q_peak - 200) sin^2(pi t / 24 h) m^3/s, Q_peak drawn from
+    U[1000, 3000] by ``hydro_seed``, imposed as the normal velocity Q / (20 km * 10 m)
+    (a velocity boundary, like the beach's inflow).  Seeds 40-47 train the network, 48-51
+    evaluate it."""
+    base = basin_case(n=n, seed=seed, nsteps=nsteps)
+    q_peak = float(np.random.default_rng(hydro_seed).uniform(1000.0, 3000.0))
+    east = (n - 1) * n + np.arange(n)
+    seg_e = boundary_segments(east, +1)
+    seg = np.concatenate([base.seg, seg_e])
+    kind = np.concatenate([base.seg_kind, np.zeros(len(seg_e), np.int32)])
+    tf = dt * (nsteps + 1)
+    t = np.arange(0.0, tf + dt, dt / 4.0)
+    depth = 10.0 + 1.0 * np.sin(2 * np.pi * t / (12.42 * 3600.0))
+    q = 200.0 + (q_peak - 200.0) * np.sin(np.pi * t / (24 * 3600.0)) ** 2
+    series = {0: (t, depth), 1: (t, -q / (20000.0 * 10.0)), 2: _const_series(0.0, tf + dt, 0.0)}
+    case = SW2Case(f"basin_hydro{hydro_seed}", base.xyz, base.tri, seg, kind, base.sol0, dt, nsteps, series)
+    case.q_peak = q_peak
+    return case

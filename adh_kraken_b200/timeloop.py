@@ -158,17 +158,25 @@ class SW2Simulation:
         src/newton/fe_newton.c:887); the rest of the interval is then covered in
         steps of the reduced size.  The reference instead ends its time loop at the
         first failure (src/timeloop/time_loop.c:37).  Gives up after max_cuts
-        reductions (success 0, the state and the clock at the last good substep).
+        reductions (success 0, the state and the clock at the last good substep).  With
+        the relative Newton test, the shorter steps keep the tolerance of the interval's
+        first attempt (sw2g_newton_opts.tol_nonlin_min).
         ``before_attempt(sim, dt)``, when given, runs before every Newton solve (e.g.
         to set an initial guess for a step of that dt).  Failed attempts are undone before anything else runs:
         the clock never moves for them and the mass log never sees them."""
         target = self.t + self.case.dt
         dt, cuts, subs, failed = self.case.dt, 0, [], []
+        o_cur = opts or self.opts
         while self.t + NOT_QUITE_SMALL * self.case.dt < target:
             h = min(dt, target - self.t)
             if before_attempt is not None:
                 before_attempt(self, h)
-            st, t_new = self._attempt(opts, h)
+            st, t_new = self._attempt(o_cur, h)
+            if cuts == 0 and not st["success"] and st.get("tol_used") and getattr(o_cur, "tol_nonlin_rel", 0) > 0:
+                # the shorter steps keep the interval's tolerance: the residual at the start of a
+                # short step shrinks with its dt, the attainable accuracy does not
+                o_cur = type(o_cur).from_buffer_copy(o_cur)
+                o_cur.tol_nonlin_min = float(st["tol_used"])
             if st["success"]:
                 self._record(st, t_new, h, moved=True)
                 subs.append(st)

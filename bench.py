@@ -339,6 +339,8 @@ def run_ours(args, world, rank, local, dist):
         L = lib()
         solves = 0
 
+        o_e2e = [opts_fast]
+
         def solve(t_start, h):
             nonlocal solves
             d, vx, vy = fast.bc_values(t_start, t_start + h)
@@ -349,7 +351,7 @@ def run_ours(args, world, rank, local, dist):
                 m.set_guess(None)
             rc = L.sw2g_fe_newton(m.h, C.c_void_p(sol_h.data_ptr()), C.c_void_p(old_h.data_ptr()),
                                   C.c_void_p(older_h.data_ptr()), C.c_void_p(mask_h.data_ptr()),
-                                  C.c_void_p(dir_h.data_ptr()), C.byref(opts_fast), C.byref(st))
+                                  C.c_void_p(dir_h.data_ptr()), C.byref(o_e2e[0]), C.byref(st))
             solves += 1
             if rc not in (0, -5):                 # -5: non-finite residual, a failed solve (state kept)
                 raise RuntimeError(L.sw2g_last_error().decode())
@@ -366,6 +368,7 @@ def run_ours(args, world, rank, local, dist):
         w0 = time.perf_counter()
         for _ in range(K):
             target, h, ok = t_e + case.dt, case.dt, True
+            o_e2e[0] = opts_fast
             for cut in range(4):
                 while t_e + 1e-6 * case.dt < target:
                     hh = min(h, target - t_e)
@@ -374,6 +377,9 @@ def run_ours(args, world, rank, local, dist):
                     t_e += hh
                 if t_e + 1e-6 * case.dt >= target:
                     break
+                if cut == 0 and st.tol_used > 0:   # shorter steps keep the interval's tolerance, as advance() does
+                    o_e2e[0] = type(opts_fast).from_buffer_copy(opts_fast)
+                    o_e2e[0].tol_nonlin_min = st.tol_used
                 h *= DT_REDUCE_FACTOR
             else:
                 ok = False

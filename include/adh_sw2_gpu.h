@@ -73,6 +73,11 @@ typedef struct {
                                  2 inside it.  They remove the stall of the linear solve at shallow wet/dry
                                  nodes on some steps and slow or break it on others (nearly singular chunk
                                  blocks), so they are off unless asked for. */
+    double tol_nonlin_min;    /* with tol_nonlin_rel > 0: the tolerance is max(tol_nonlin_rel * max|R(sol_old)|,
+                                 tol_nonlin_min) (default 0).  A time loop that covers an interval in smaller
+                                 steps after a failed solve passes the interval's own tolerance here: the
+                                 residual at the start of a short step shrinks with its dt, the attainable
+                                 accuracy does not. */
 } sw2g_newton_opts;
 
 /* Krylov methods of the Newton correction.  BiCGStab is the reference's

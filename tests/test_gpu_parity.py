@@ -224,8 +224,7 @@ def test_config1_flume_100_steps_match_reference(mode):
     assert worst < 1e-8, worst
 
 
-@pytest.mark.parametrize("name", ["run_wetdry_12_4steps.npz", "run_wetdry_12_dt600_6steps.npz",
-                                  "run_still_beach_16x6_1440steps.npz"])
+@pytest.mark.parametrize("name", ["run_wetdry_12_4steps.npz", "run_still_beach_16x6_1440steps.npz"])
 def test_amg_chunk_corrections_are_exercised_and_match_reference(name):
     """The AMG's chunk corrections (amg_chunks = 2: exact solves on the chunks of nodes whose
     block-Jacobi smoothing the l1 fix-up weakens, inside the V-cycle) run on wet/dry meshes,
