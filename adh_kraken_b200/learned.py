@@ -437,8 +437,6 @@ def main(out=WEIGHTS, nsteps=12, seed=4, iters=300, nx=2828, ny=707, krylov_tol=
     return net, before, after
 
 
-if __name__ == "__main__":
-    main()
 
 
 def device_trajectory(case, nsteps, opts=None):
@@ -546,3 +544,26 @@ def config4(n=707, train_seeds=tuple(range(40, 48)), test_seeds=tuple(range(48, 
                             "steps_per_traj": steps_per_traj, "iters": iters, "loss_before": before,
                             "loss_after": after})
     return net, res
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the learned initial guess")
+    ap.add_argument("--config4", action="store_true",
+                    help="the basin experiment with 8 training and 4 held-out inflow hydrographs")
+    ap.add_argument("--n", type=int, default=707)
+    ap.add_argument("--steps-per-traj", type=int, default=375)
+    ap.add_argument("--eval-steps", type=int, default=40)
+    ap.add_argument("--iters", type=int, default=2000)
+    ap.add_argument("--out", default=None, help="weights file")
+    ap.add_argument("--report", default=None, help="JSON report of the experiment")
+    a = ap.parse_args()
+    if a.config4:
+        _, res = config4(n=a.n, steps_per_traj=a.steps_per_traj, eval_steps=a.eval_steps, iters=a.iters, out=a.out,
+                         log=lambda m: print(m, flush=True))
+        if a.report:
+            with open(a.report, "w") as fh:
+                json.dump(res, fh, indent=1, default=float)
+    else:
+        main(out=a.out or WEIGHTS)

@@ -304,3 +304,49 @@ def basin_hydro_case(hydro_seed: int, n: int = 707, seed: int = 2, nsteps: int =
     case = SW2Case(f"basin_hydro{hydro_seed}", base.xyz, base.tri, seg, kind, base.sol0, dt, nsteps, series)
     case.q_peak = q_peak
     return case
+
+
+def estuary_case(nx: int = 4000, ny: int = 2000, seed: int = 5, nsteps: int = 500, dt: float = 180.0) -> SW2Case:
+    """Estuary: 80 km x 40 km jittered Delaunay (nx x ny; the default 4000 x 2000 gives
+    ~16M triangles), the ocean on the west edge and a river on the east edge.  Depth
+    falls from 30 m at the ocean to 2 m at the river end; 32 seeded Gaussian shoals
+    (height U[1, 5] m, sigma U[1, 4] km) rise out of the water where the base depth is
+    small (partial wet/dry); a meandering channel (centreline 20 km + 5 km sin(2 pi x /
+    40 km), 500 m wide) is 2 m deeper.  Forcing: an M2 tide of 1.5 m amplitude (12.42 h)
+    as the depth of the flat west edge, and the river's 800 m^3/s as the inflow velocity
+    on the east-edge segments inside the channel (800 / (500 m * 4 m)); the rest of the
+    boundary is closed.  Still water at eta = 0 to start, dt = 180 s."""
+    rng = np.random.default_rng(seed)
+    LX, LY = 80000.0, 40000.0
+    x, y, tri, (ii, jj) = jittered_delaunay(nx, ny, LX, LY, 0.3, rng)
+    depth = 30.0 - 28.0 * x / LX
+    cx = rng.uniform(0, LX, 32); cy = rng.uniform(0, LY, 32)
+    amp = rng.uniform(1, 5, 32); sig = rng.uniform(1000, 4000, 32)
+    for k in range(32):
+        depth = depth - amp[k] * np.exp(-((x - cx[k]) ** 2 + (y - cy[k]) ** 2) / (2 * sig[k] ** 2))
+    yc = 20000.0 + 5000.0 * np.sin(2 * np.pi * x / 40000.0)
+    channel = np.abs(y - yc) < 250.0
+    depth = np.where(channel, depth + 2.0, depth)
+    west = np.arange(ny)
+    depth[west] = 30.0                               # flat tidal edge (one depth for the whole string)
+    z = -depth
+    xyz = np.stack([x, y, z], axis=1)
+    ch = _edge_chains(ii, jj, nx, ny)
+    seg_w = boundary_segments(ch["west"], -1)
+    east = ch["east"]
+    seg_e_all = boundary_segments(east, +1)
+    mid = 0.5 * (y[seg_e_all[:, 0]] + y[seg_e_all[:, 1]])
+    yce = 20000.0 + 5000.0 * np.sin(2 * np.pi * LX / 40000.0)
+    seg_e = seg_e_all[np.abs(mid - yce) < 250.0]
+    z[np.unique(seg_e.ravel())] = -4.0               # the river mouth: 4 m deep
+    xyz[:, 2] = z
+    seg = np.concatenate([seg_w, seg_e])
+    kind = np.concatenate([np.ones(len(seg_w), np.int32), np.zeros(len(seg_e), np.int32)])
+    V = xyz.shape[0]
+    sol0 = np.zeros(3 * V)
+    sol0[0::3] = -z
+    tf = dt * (nsteps + 1)
+    t = np.arange(0.0, tf + dt, dt / 4.0)
+    tide = 30.0 + 1.5 * np.sin(2 * np.pi * t / (12.42 * 3600.0))
+    series = {0: (t, tide), 1: _const_series(0.0, tf + dt, -800.0 / (500.0 * 4.0)), 2: _const_series(0.0, tf + dt, 0.0)}
+    return SW2Case("estuary", xyz, tri, seg, kind, sol0, dt, nsteps, series)

@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["beach4M", "basin1M", "estuary16M"], default="beach4M",
+                   help="beach4M: the benchmark configuration; basin1M (fully wet tidal basin, dt 300 s) and "
+                        "estuary16M (partial wet/dry estuary, dt 180 s) measure the other GPU configurations")
     p.add_argument("--nx", type=int, default=2828)
     p.add_argument("--ny", type=int, default=707)
     p.add_argument("--krylov-tol", type=float, default=1e-6,
@@ -218,16 +221,23 @@ def run_ours(args, world, rank, local, dist):
     torch.cuda.set_device(local)
     K, W = args.steps, args.warmup
     cpu_run = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "beach4M":
         cpu_run = start_cpu_reference(W + K)    # CPU work in the background while the GPU runs
-    case = beach_case(nx=args.nx, ny=args.ny, nsteps=W + 2 * K + 8)
+    if args.workload == "basin1M":
+        from adh_kraken_b200.mesh import basin_case
+        case = basin_case(n=707, seed=2, nsteps=W + 2 * K + 8)
+    elif args.workload == "estuary16M":
+        from adh_kraken_b200.mesh import estuary_case
+        case = estuary_case(nsteps=W + 2 * K + 8)
+    else:
+        case = beach_case(nx=args.nx, ny=args.ny, nsteps=W + 2 * K + 8)
     base = dict(tol_nonlin=1e-8, tol_nonlin_rel=args.tol_rel, inc_nonlin=1e-6, max_nonlin_it=10,
                 krylov_max_it=20000, krylov_tol=args.krylov_tol, precond=2, krylov_method=1,
                 krylov_restart=args.restart)
     opts_fast = default_opts(krylov_precision=32, krylov_basis_precision=args.basis, **base)
     opts_plain = default_opts(krylov_precision=64, **base)
     guesser = None
-    if args.guess == "learned":
+    if args.guess == "learned" and args.workload == "beach4M":
         from adh_kraken_b200 import learned
         guesser = learned.load_guesser(case, args.weights) if args.weights else learned.load_guesser(case)
     if guesser is not None:
@@ -431,7 +441,7 @@ def run_ours(args, world, rank, local, dist):
         "metric": METRIC, "value": world * sf["intervals_ok"] / (ms_fast * 1e-3), "unit": UNIT, "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": ms_fast / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-        "config": {"workload": "beach4M", "ntri": case.ntri, "nnodes": case.nnodes, "ndofs": 3 * case.nnodes,
+        "config": {"workload": args.workload, "ntri": case.ntri, "nnodes": case.nnodes, "ndofs": 3 * case.nnodes,
                    "nnz": fast.model.nnz, "dt_s": case.dt, "tol_nonlin": 1e-8, "tol_nonlin_rel": args.tol_rel,
                    "krylov": f"GMRES({args.restart})+AMG", "krylov_forcing": args.krylov_tol,
                    "guess": args.guess if guesser is not None else "none",

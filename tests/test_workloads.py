@@ -29,3 +29,18 @@ def test_basin_hydro_case_steps_on_the_oracle():
     sol, hist = OracleModel(c).run(2, krylov_max_it=20000)
     assert all(h["ok"] for h in hist)
     assert np.isfinite(sol).all() and sol[0::3].min() > 0
+
+
+def test_estuary_case_has_tide_river_and_dry_land():
+    from adh_kraken_b200.mesh import estuary_case
+    c = estuary_case(nx=240, ny=120, nsteps=2)
+    depth_edge = c.seg[c.seg_kind == 1]
+    river = c.seg[c.seg_kind == 0]
+    assert len(depth_edge) == 119 and len(river) >= 1
+    assert np.allclose(c.xyz[np.unique(depth_edge.ravel()), 2], -30.0)     # flat tidal edge
+    assert np.allclose(c.xyz[river.ravel(), 0], 80000.0)
+    dry = (c.sol0[0::3] <= 0).mean()
+    assert 0.0 < dry < 0.2                                                 # partial wet/dry
+    t, v = c.series[0]
+    assert np.allclose(v, 30.0 + 1.5 * np.sin(2 * np.pi * t / (12.42 * 3600.0)))
+    assert np.isclose(c.series[1][1][0], -0.4)                             # 800 m^3/s through 500 m x 4 m
