@@ -55,7 +55,7 @@ struct sw2g_model {
     // mesh
     int *d_tri = nullptr, *d_seg = nullptr, *d_skind = nullptr;
     double *d_ex = nullptr, *d_ey = nullptr, *d_ez = nullptr, *d_gx = nullptr, *d_gy = nullptr, *d_djac = nullptr;
-    double *d_snx = nullptr, *d_sny = nullptr, *d_sdjac = nullptr;
+    double *d_snx = nullptr, *d_sny = nullptr, *d_sdjac = nullptr, *d_sz0 = nullptr;
     // CSR and node blocks
     int *d_indptr = nullptr, *d_cols = nullptr, *d_bptr = nullptr, *d_bcol = nullptr, *d_diag = nullptr;
     // assembly maps
@@ -217,6 +217,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
     if ((long)(T + S) * 9 >= (1L << 31) || 3L * V >= (1L << 31)) { g_err = "sw2g_create: mesh too large for 32-bit maps"; return SW2G_ERR_ARG; }
     for (long i = 0; i < 3L * T; i++) if (mesh->tri[i] < 0 || mesh->tri[i] >= V) { g_err = "sw2g_create: triangle node id out of range"; return SW2G_ERR_MESH; }
     for (long i = 0; i < 2L * S; i++) if (mesh->seg[i] < 0 || mesh->seg[i] >= V) { g_err = "sw2g_create: segment node id out of range"; return SW2G_ERR_MESH; }
+    for (int i = 0; i < S; i++) if (mesh->seg_kind[i] < 0 || mesh->seg_kind[i] > 3) { g_err = "sw2g_create: segment kind not in 0..3"; return SW2G_ERR_ARG; }
     sw2g_model* m = new sw2g_model();
     m->V = V; m->T = T; m->S = S; m->Etot = T + S; m->n = 3 * V;
     if (cudaGetDevice(&m->device) != cudaSuccess) { g_err = "sw2g_create: no current CUDA device"; delete m; return SW2G_ERR_CUDA; }
@@ -248,10 +249,11 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         dj[e] = djac * (1.0 / 2.0);
         if (!(dj[e] > 1e-6)) { g_err = "sw2g_create: triangle not counter-clockwise (selem2d_load rejects it)"; return fail(SW2G_ERR_MESH); }
     }
-    std::vector<double> snx(S + 1), sny(S + 1), sdj(S + 1);
+    std::vector<double> snx(S + 1), sny(S + 1), sdj(S + 1), sz0(S + 1, 0.0);
     for (int k = 0; k < S; k++) {
         const double* a = mesh->xyz + 3 * (size_t)mesh->seg[2 * k];
         const double* b = mesh->xyz + 3 * (size_t)mesh->seg[2 * k + 1];
+        sz0[k] = a[2];
         double d = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]));
         if (!(d > 1e-6)) { g_err = "sw2g_create: zero-length boundary segment"; return fail(SW2G_ERR_MESH); }
         sdj[k] = d; snx[k] = (b[1] - a[1]) / d; sny[k] = -(b[0] - a[0]) / d;
@@ -366,7 +368,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         (rc = upload(m, &m->d_ez, ez.data(), ez.size())) || (rc = upload(m, &m->d_gx, gx.data(), gx.size())) ||
         (rc = upload(m, &m->d_gy, gy.data(), gy.size())) || (rc = upload(m, &m->d_djac, dj.data(), dj.size())) ||
         (rc = upload(m, &m->d_snx, snx.data(), snx.size())) || (rc = upload(m, &m->d_sny, sny.data(), sny.size())) ||
-        (rc = upload(m, &m->d_sdjac, sdj.data(), sdj.size())))
+        (rc = upload(m, &m->d_sdjac, sdj.data(), sdj.size())) || (rc = upload(m, &m->d_sz0, sz0.data(), sz0.size())))
         return fail(rc);
     if ((rc = upload(m, &m->d_indptr, ip.data(), ip.size())) || (rc = upload(m, &m->d_cols, cl.data(), cl.size())) ||
         (rc = upload(m, &m->d_bptr, bptr.data(), bptr.size())) || (rc = upload(m, &m->d_bcol, bcol.data(), bcol.size())) ||
@@ -402,10 +404,10 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
         g_err = "cudaMallocHost failed"; return fail(SW2G_ERR_NOMEM);
     }
     m->M = MeshView{V, T, S, m->d_tri, m->d_ex, m->d_ey, m->d_ez, m->d_gx, m->d_gy, m->d_djac,
-                    m->d_seg, m->d_snx, m->d_sny, m->d_sdjac, m->d_skind};
+                    m->d_seg, m->d_snx, m->d_sny, m->d_sdjac, m->d_skind, m->d_sz0};
     m->A = AssemblyMaps{m->nslots, m->d_rptr, m->d_rmap, m->d_jptr, m->d_jmap, m->d_boff, m->d_blen};
     m->B = BlockCSR{V, m->n, m->nnz, m->d_indptr, m->d_cols, m->d_bptr, m->d_bcol, m->d_diag};
-    m->P = StepParams{1.0, 0.0, mesh->gravity, 0.0, 0.0, 0.0};
+    m->P = StepParams{1.0, 0.0, mesh->gravity, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0};
     CK(cudaStreamSynchronize(m->st));
     *out = m;
     return SW2G_OK;
@@ -461,6 +463,16 @@ extern "C" int sw2g_get_sparsity(const sw2g_model* m, int* indptr, int* cols) {
 extern "C" int sw2g_set_step(sw2g_model* m, double dt, double tau, double bc_depth, double bc_vx, double bc_vy) {
     if (!m || !(dt > 0)) { g_err = "sw2g_set_step: bad model or dt"; return SW2G_ERR_ARG; }
     m->P.dt = dt; m->P.alpha = tau; m->P.bc_depth = bc_depth; m->P.bc_vx = bc_vx; m->P.bc_vy = bc_vy;
+    return SW2G_OK;
+}
+extern "C" int sw2g_set_bc_structures(sw2g_model* m, double q_series, double conveyance, double rough_height,
+                                      double tail_elev) {
+    if (!m) { g_err = "sw2g_set_bc_structures: null model"; return SW2G_ERR_ARG; }
+    if (!std::isfinite(q_series) || !std::isfinite(conveyance) || !std::isfinite(rough_height) || !std::isfinite(tail_elev)) {
+        g_err = "sw2g_set_bc_structures: non-finite value"; return SW2G_ERR_ARG;
+    }
+    if (conveyance == 0.0) { g_err = "sw2g_set_bc_structures: zero conveyance"; return SW2G_ERR_ARG; }
+    m->P.bc_qs = q_series; m->P.bc_convey = conveyance; m->P.bc_rough = rough_height; m->P.bc_tail = tail_elev;
     return SW2G_OK;
 }
 extern "C" void* sw2g_stream(sw2g_model* m) { return m ? (void*)m->st : nullptr; }

@@ -487,8 +487,79 @@ __device__ __forceinline__ void body_resid(const TriData& T, double dt, double a
 struct SegData {
     V2 n; double djac;
     double h[2]; V2 vel[2];
-    int kind;   // 0 velocity (fe_sw2_bc_vel), 1 depth (fe_sw2_bc_h)
+    double z0;  // bed elevation of the segment's first node
+    int kind;   // 0 velocity (fe_sw2_bc_vel), 1 depth (fe_sw2_bc_h), 2 discharge, 3 tailwater
 };
+
+// The boundary values of one step, shared by every segment of a kind.
+struct SegBC {
+    double depth, vx, vy;   // series 0, 1, 2: fe_sw2_bc_h's depth, fe_sw2_bc_vel's velocity
+    double q_series;        // discharge string's series value (sw2_bc_discharge.c.bk:161)
+    double conveyance;      // discharge string's conveyance (sstr_value.h:63)
+    double rough_height;    // equivalent roughness height of the boundary strings (FRICTION.eqrheight)
+    double tail_elev;       // tailwater elevation series value (sw2_bc_tailwater.c.bk:154)
+};
+
+// fr_bedshstr_drag_coef, src/friction/fr_bedshstr_drag_coef.c:18-42
+__device__ __forceinline__ double bedshstr_drag_coef(double depth, double rh) {
+    depth = depth > 1.E-8 ? depth : 1.E-8;
+    rh = rh > 1.E-8 ? rh : 1.E-8;
+    double depth_rh = (rh > 29.7 * depth) ? 1. / 29.7 : depth / rh;
+    double bta = 29.7 * depth_rh;
+    double phi = pow((.4 * bta) / ((bta + 1) * (log(bta + 1) - 1) + 1), 2.);
+    return 2. * phi;
+}
+
+// fe_sw2_get_roughness (src/models/sw2/sw2_get_roughness.c:24-49) for a string with
+// neither vegetation nor ice: the bed-shear drag of its roughness height, else zero drag
+__device__ __forceinline__ double bc_roughness(double depth, double rh) {
+    return rh > SW2_SMALL ? bedshstr_drag_coef(depth, rh) : 0.0;
+}
+
+// integrate_line_phi (src/fe/fe_integrals_1d.c:54)
+__device__ __forceinline__ void line_phi(double djac, double c, double q[2]) {
+    double t1 = SW2_ONE_2 * djac * c;
+    q[0] += t1; q[1] += t1;
+}
+
+// integrate_line_phi_f (src/fe/fe_integrals_1d.c:67)
+__device__ __forceinline__ void line_phi_f(double djac, double c, const double f[2], double q[2]) {
+    double t1 = SW2_ONE_6 * djac * c;
+    q[0] += t1 * (2 * f[0] + f[1]);
+    q[1] += t1 * (f[0] + 2 * f[1]);
+}
+
+// fe_sw2_1d_explicit_flow, src/fe/fe_sw2_boundary_integrals.c:56-82 (flux < 0 is inflow)
+__device__ __forceinline__ void explicit_flow(double r[6], V2 n, double djac, double dt, double flux, double h_avg,
+                                              const double u[2], const double v[2]) {
+    double rc[2] = {0., 0.}, rx[2] = {0., 0.}, ry[2] = {0., 0.};
+    line_phi(djac, 1., rc);
+    if (flux < 0) {
+        double u_star = 0., v_star = 0.;
+        if (h_avg > 0) {
+            u_star = flux * n.x / h_avg;
+            v_star = flux * n.y / h_avg;
+        }
+        line_phi(djac, u_star, rx);
+        line_phi(djac, v_star, ry);
+    } else {
+        line_phi_f(djac, 1., u, rx);
+        line_phi_f(djac, 1., v, ry);
+    }
+    double t1 = dt * flux;
+#pragma unroll
+    for (int i = 0; i < 2; i++) { r[i * 3] += t1 * rc[i]; r[i * 3 + 1] += t1 * rx[i]; r[i * 3 + 2] += t1 * ry[i]; }
+}
+
+// fe_sw2_1d_wall_friction, src/fe/fe_sw2_boundary_integrals.c:205-219
+__device__ __forceinline__ void wall_friction(double r[6], V2 n, double djac, double dt, const double u[2],
+                                              const double v[2], const double res[2]) {
+    double rx[2] = {0., 0.}, ry[2] = {0., 0.};
+    line_phi_f(djac, fabs(n.y), u, rx);
+    line_phi_f(djac, fabs(n.x), v, ry);
+#pragma unroll
+    for (int i = 0; i < 2; i++) { r[i * 3 + 1] += dt * res[i] * rx[i]; r[i * 3 + 2] += dt * res[i] * ry[i]; }
+}
 
 // fe_sw2_1d_implicit_flow, src/fe/fe_sw2_boundary_integrals.c:125
 __device__ __forceinline__ void implicit_flow(double r[6], V2 n, double djac, double dt, const V2 v[2], const double h[2]) {
@@ -521,17 +592,41 @@ __device__ __forceinline__ void pressure_1d(double r[6], V2 n, double djac, doub
 }
 
 template <bool PRESSURE>
-__device__ __forceinline__ void seg_resid(const SegData& S, double dt, double grav, double bc_depth, double bc_vx,
-                                          double bc_vy, double r[6]) {
+__device__ __forceinline__ void seg_resid(const SegData& S, double dt, double grav, const SegBC& B, double r[6]) {
 #pragma unroll
     for (int i = 0; i < 6; i++) r[i] = 0.0;
     if (S.kind == 0) {   // sw2_bc_vel.c:147-159: the boundary velocity replaces u, v
-        V2 v[2] = {{bc_vx, bc_vy}, {bc_vx, bc_vy}};
+        V2 v[2] = {{B.vx, B.vy}, {B.vx, B.vy}};
         implicit_flow(r, S.n, S.djac, dt, v, S.h);
-    } else {             // sw2_bc_h.c:150-172
-        double dep[2] = {bc_depth, bc_depth};
+    } else if (S.kind == 1) {   // sw2_bc_h.c:150-172
+        double dep[2] = {B.depth, B.depth};
         if (dep[0] < SW2_SMALL || dep[1] < SW2_SMALL || S.h[0] < SW2_SMALL || S.h[1] < SW2_SMALL) return;
         implicit_flow(r, S.n, S.djac, dt, S.vel, dep);
+        if (PRESSURE) {
+            pressure_1d(r, S.n, S.djac, dt, dep, grav);
+            pressure_1d(r, S.n, S.djac, dt, S.h, -grav);
+        }
+    } else if (S.kind == 2) {   // sw2_bc_discharge.c.bk:111-172
+        double u_tan = SW2_ONE_2 * (S.vel[0].x + S.vel[1].x) * S.n.y - SW2_ONE_2 * (S.vel[0].y + S.vel[1].y) * S.n.x;
+        double mag_utan = fabs(u_tan);
+        double u[2] = {S.vel[0].x, S.vel[1].x}, v[2] = {S.vel[0].y, S.vel[1].y};
+        double h_avg = SW2_ONE_2 * (S.h[0] + S.h[1]);
+        if (h_avg < SW2_SMALL) h_avg = SW2_SMALL;
+        double res[2] = {SW2_ONE_2 * bc_roughness(S.h[0], B.rough_height) * mag_utan,
+                         SW2_ONE_2 * bc_roughness(S.h[1], B.rough_height) * mag_utan};
+        if (S.h[0] < SW2_SMALL || S.h[1] < SW2_SMALL) return;
+        // the discharge law takes the first node's head at both nodes (.bk:164-167)
+        double fact = -1.0 * B.q_series * sqrt(2. * grav / bc_roughness(S.h[0], B.rough_height)) / B.conveyance;
+        double d0 = fact * pow(S.h[0], 1.5);
+        fact = -1.0 * B.q_series * sqrt(2. * grav / bc_roughness(S.h[1], B.rough_height)) / B.conveyance;
+        double d1 = fact * pow(S.h[0], 1.5);
+        explicit_flow(r, S.n, S.djac, dt, SW2_ONE_2 * (d0 + d1), h_avg, u, v);
+        wall_friction(r, S.n, S.djac, dt, u, v, res);
+    } else {                    // kind 3: sw2_bc_tailwater.c.bk:152-170
+        // depth below the tailwater elevation at the first node, used at both nodes (.bk:155-156)
+        double dep[2] = {B.tail_elev - S.z0, B.tail_elev - S.z0};
+        if (dep[0] < SW2_SMALL || dep[1] < SW2_SMALL || S.h[0] < SW2_SMALL || S.h[1] < SW2_SMALL) return;
+        implicit_flow(r, S.n, S.djac, dt, S.vel, S.h);
         if (PRESSURE) {
             pressure_1d(r, S.n, S.djac, dt, dep, grav);
             pressure_1d(r, S.n, S.djac, dt, S.h, -grav);

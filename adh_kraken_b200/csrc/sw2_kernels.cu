@@ -38,8 +38,12 @@ __device__ __forceinline__ void load_tri(const MeshView& M, const double* __rest
     T.wd_flag = wd_flag[e];
 }
 
+__device__ __forceinline__ SegBC seg_bc(const StepParams& P) {
+    return SegBC{P.bc_depth, P.bc_vx, P.bc_vy, P.bc_qs, P.bc_convey, P.bc_rough, P.bc_tail};
+}
+
 __device__ __forceinline__ void load_seg(const MeshView& M, const double* __restrict__ sol, int s, SegData& S) {
-    S.n.x = M.snx[s]; S.n.y = M.sny[s]; S.djac = M.sdjac[s]; S.kind = M.skind[s];
+    S.n.x = M.snx[s]; S.n.y = M.sny[s]; S.djac = M.sdjac[s]; S.kind = M.skind[s]; S.z0 = M.sz0[s];
 #pragma unroll
     for (int a = 0; a < 2; a++) {
         const int n = M.seg[2 * s + a];
@@ -100,7 +104,7 @@ __global__ void k_resid_seg(MeshView M, StepParams P, const double* __restrict__
     SegData S;
     load_seg(M, sol, s, S);
     double r[6];
-    seg_resid<true>(S, P.dt, P.grav, P.bc_depth, P.bc_vx, P.bc_vy, r);
+    seg_resid<true>(S, P.dt, P.grav, seg_bc(P), r);
     double* out = ER + 9 * ((size_t)M.ntri + s);
 #pragma unroll
     for (int i = 0; i < 6; i++) out[i] = r[i];
@@ -171,13 +175,14 @@ __global__ void k_fd_seg(MeshView M, StepParams P, const double* __restrict__ so
     double u0 = k == 0 ? S.h[i] : (k == 1 ? S.vel[i].x : S.vel[i].y);
     const double eps = fd_eps(u0);
     const double eps2 = 2.0 * eps;
+    const SegBC B = seg_bc(P);
     double Rp[6], Rm[6];
     for (int sgn = 0; sgn < 2; sgn++) {
         SegData Q = S;
         const double d = (sgn == 0 ? 1 : -1) * eps;
         if (k == 0) Q.h[i] += d; else if (k == 1) Q.vel[i].x += d; else Q.vel[i].y += d;
-        if (k == 0) seg_resid<true>(Q, P.dt, P.grav, P.bc_depth, P.bc_vx, P.bc_vy, sgn == 0 ? Rp : Rm);
-        else seg_resid<false>(Q, P.dt, P.grav, P.bc_depth, P.bc_vx, P.bc_vy, sgn == 0 ? Rp : Rm);
+        if (k == 0) seg_resid<true>(Q, P.dt, P.grav, B, sgn == 0 ? Rp : Rm);
+        else seg_resid<false>(Q, P.dt, P.grav, B, sgn == 0 ? Rp : Rm);
     }
     double* out = EJ + ((size_t)col * Etot + M.ntri + s) * 9;
     for (int r = 0; r < 6; r++) out[r] = (Rp[r] - Rm[r]) / eps2;

@@ -31,6 +31,8 @@ H = 64
 LAYERS = [(8, H), (4 * H, H), (4 * H, H), (4 * H, H), (H, 3)]   # (in, out): encoder, 3 layers, decoder
 MIN_DEPTH = 0.05   # m: nodes this shallow keep the previous step in the guess
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "beach_guess.npz")
+# trained by config4() on the basin with inflow hydrographs (n = 707, 8 x 375 steps, 2000 iterations)
+BASIN_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "basin_guess.npz")
 
 _GNN_FUNCS = ["sw2n_agg_fwd", "sw2n_agg_bwd", "sw2n_dense_fwd", "sw2n_dense_bwd", "sw2n_adam", "sw2n_to_bf16",
               "sw2n_features", "sw2n_targets", "sw2n_mse", "sw2n_apply_guess", "sw2n_smooth3", "sw2n_smooth3_adj"]
@@ -464,28 +466,43 @@ def device_trajectory(case, nsteps, opts=None):
     return tr
 
 
-def evaluate_guess(net, case, nsteps, opts):
-    """Runs ``nsteps`` steps of ``case`` twice from its initial state: Newton started from
+def evaluate_guess(net, case, nsteps, opts, start=0):
+    """Runs ``nsteps`` steps of ``case`` twice from the same state: Newton started from
     the previous step (the reference's start) and from the network's guess (use_guess = 1;
-    the residual still judges it).  Per run: Newton and Krylov iterations, steps the guess
-    started, and device time (CUDA events on the model's stream, guess inference
-    included)."""
+    the residual still judges it).  With ``start`` > 0 both runs begin after ``start``
+    spin-up steps taken once from the initial state with the previous-step start.  Per
+    run: Newton and Krylov iterations, steps the guess started, and device time (CUDA
+    events on the model's stream, guess inference included)."""
     import copy
     import torch
     from .timeloop import SW2Simulation
-    out = {}
+    s0, t0 = None, case.t0
+    if start > 0:
+        o = copy.copy(opts)
+        o.use_guess = 0
+        sim = SW2Simulation(case, opts=o)
+        for _ in range(start):
+            st = sim.step()
+            if not st["success"]:
+                raise RuntimeError(f"spin-up step at t = {sim.t} did not converge")
+        s0, t0 = sim.state(), sim.t
+        sim.model.close()
+    out = {"start_step": start}
     for mode in ("previous_step", "learned"):
         o = copy.copy(opts)
         o.use_guess = 1 if mode == "learned" else 0
         sim = SW2Simulation(case, opts=o)
+        if s0 is not None:
+            sim.model.load_state(*s0[:3], bc_mask=s0[3])
+            sim.t = t0
         g = Guesser(net, case) if mode == "learned" else None
         s = torch.cuda.ExternalStream(sim.model.stream)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         rec = {"newton_its": 0, "krylov_its": 0, "guess_used": 0, "failed": 0, "steps": 0}
         torch.cuda.synchronize()
         ev0.record(s)
-        for _ in range(nsteps):
-            if g is not None and len(sim.history) > 0:    # the guess needs two states
+        for k in range(nsteps):
+            if g is not None and (k > 0 or s0 is not None):   # the guess needs two states
                 g.predict_into(sim)
             st = sim.step()
             rec["newton_its"] += st["newton_its"]; rec["krylov_its"] += st["krylov_its"]
@@ -507,42 +524,47 @@ def evaluate_guess(net, case, nsteps, opts):
 
 
 def config4(n=707, train_seeds=tuple(range(40, 48)), test_seeds=tuple(range(48, 52)), steps_per_traj=375,
-            eval_steps=40, iters=2000, out=None, opts=None, log=print):
+            eval_steps=40, iters=2000, out=None, opts=None, log=print, eval_start=0, net=None):
     """The learned-guess experiment on the basin with inflow hydrographs
     (mesh.basin_hydro_case): trajectories of the solver under the training hydrographs
     (8 x 375 = 3000 steps at the default sizes), the network trained on them by the
     library's kernels, then Newton / Krylov work and device time on the held-out
-    hydrographs with and without the learned guess."""
+    hydrographs with and without the learned guess, from step ``eval_start`` of each
+    held-out run (the hydrographs rise from base flow, so windows later in the day
+    see the different peaks).  A given ``net`` (already trained) skips the training."""
     import time
     from .capi import default_opts
     from .mesh import basin_hydro_case
     opts = opts or default_opts(precond=2, krylov_method=1, krylov_precision=32, krylov_basis_precision=32,
                                 krylov_tol=1e-6, tol_nonlin_rel=1e-8, krylov_max_it=20000, krylov_restart=50)
     t0 = time.time()
-    trajs = []
-    for sd in train_seeds:
-        case = basin_hydro_case(sd, n=n, nsteps=steps_per_traj + 2)
-        trajs.append(device_trajectory(case, steps_per_traj, opts))
-        log(f"trajectory {sd}: {len(trajs[-1])} states, {time.time() - t0:.0f} s")
-    graph = DeviceGraph(build_graph(case.xyz[:, :2], case.tri))
-    net = Net()
-    set_normalisation(net, trajs, stride=max(1, steps_per_traj // 25))
-    before = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
-    losses = train(net, graph, trajs, iters=iters, log_every=max(1, iters // 10))
-    after = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
-    log(f"trained {iters} iterations: loss {before:.4f} (linear extrapolation) -> {after:.4f}, {time.time() - t0:.0f} s")
-    del trajs
-    res = {"train_states": sum(1 for _ in train_seeds) * steps_per_traj, "loss_before": before, "loss_after": after,
-           "losses": losses, "held_out": {}}
+    res = {"held_out": {}}
+    if net is None:
+        trajs = []
+        for sd in train_seeds:
+            case = basin_hydro_case(sd, n=n, nsteps=steps_per_traj + 2)
+            trajs.append(device_trajectory(case, steps_per_traj, opts))
+            log(f"trajectory {sd}: {len(trajs[-1])} states, {time.time() - t0:.0f} s")
+        graph = DeviceGraph(build_graph(case.xyz[:, :2], case.tri))
+        net = Net()
+        set_normalisation(net, trajs, stride=max(1, steps_per_traj // 25))
+        before = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
+        losses = train(net, graph, trajs, iters=iters, log_every=max(1, iters // 10))
+        after = evaluate_loss(net, graph, [tr for tr in trajs[:1]])
+        log(f"trained {iters} iterations: loss {before:.4f} (linear extrapolation) -> {after:.4f}, "
+            f"{time.time() - t0:.0f} s")
+        del trajs
+        res.update({"train_states": sum(1 for _ in train_seeds) * steps_per_traj, "loss_before": before,
+                    "loss_after": after, "losses": losses})
     for sd in test_seeds:
-        case = basin_hydro_case(sd, n=n, nsteps=eval_steps + 2)
-        res["held_out"][sd] = evaluate_guess(net, case, eval_steps, opts)
+        case = basin_hydro_case(sd, n=n, nsteps=eval_start + eval_steps + 2)
+        res["held_out"][sd] = evaluate_guess(net, case, eval_steps, opts, start=eval_start)
         res["held_out"][sd]["q_peak"] = case.q_peak
         log(f"held-out {sd}: {res['held_out'][sd]}")
-    if out:
+    if out and "loss_after" in res:
         net.save(out, meta={"workload": "basin_hydro", "n": n, "train_seeds": list(train_seeds),
-                            "steps_per_traj": steps_per_traj, "iters": iters, "loss_before": before,
-                            "loss_after": after})
+                            "steps_per_traj": steps_per_traj, "iters": iters, "loss_before": res["loss_before"],
+                            "loss_after": res["loss_after"]})
     return net, res
 
 
@@ -558,10 +580,13 @@ if __name__ == "__main__":
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--out", default=None, help="weights file")
     ap.add_argument("--report", default=None, help="JSON report of the experiment")
+    ap.add_argument("--eval-start", type=int, default=0, help="spin-up steps before each held-out window")
+    ap.add_argument("--weights", default=None, help="evaluate these trained weights instead of training")
     a = ap.parse_args()
     if a.config4:
+        net = Net.load(a.weights) if a.weights else None
         _, res = config4(n=a.n, steps_per_traj=a.steps_per_traj, eval_steps=a.eval_steps, iters=a.iters, out=a.out,
-                         log=lambda m: print(m, flush=True))
+                         log=lambda m: print(m, flush=True), eval_start=a.eval_start, net=net)
         if a.report:
             with open(a.report, "w") as fh:
                 json.dump(res, fh, indent=1, default=float)

@@ -7,12 +7,16 @@ conventions:
 * boundary segments ``seg`` whose node order gives the outward normal
   (``nrml = (dy, -dx)/len`` for a segment from node 0 to node 1,
   src/structs/selem/selem_1d.c:54-55);
-* ``seg_kind`` 0 for a weak velocity boundary ("NB VEL", ``fe_sw2_bc_vel``) and 1 for
-  a weak depth boundary ("DEPTH", ``fe_sw2_bc_h``);
+* ``seg_kind`` 0 for a weak velocity boundary ("NB VEL", ``fe_sw2_bc_vel``), 1 for
+  a weak depth boundary ("DEPTH", ``fe_sw2_bc_h``), 2 for a discharge string
+  (``fe_sw2_bc_discharge``, src/models/sw2/sw2_bc_discharge.c.bk) and 3 for a
+  tailwater string (``fe_sw2_bc_tailwater``, sw2_bc_tailwater.c.bk);
 * the node-major state ``[h, u, v]`` per node (dof = 3*node + var,
   src/structs/sivar_position/sivar_position.c:61-81);
 * time series: id 0 = boundary depth (hard-coded in src/models/sw2/sw2_bc_h.c:156),
-  ids 1/2 = boundary velocity x/y.
+  ids 1/2 = boundary velocity x/y, id 3 = the discharge string's series value,
+  id 4 = the tailwater elevation; ``bc_conveyance`` and ``bc_rough_height`` are the
+  discharge string's conveyance and the boundary strings' roughness height.
 
 The structured flume reproduces the node and triangle layout of the reference's
 ``create_rectangular_grid`` (src/tools/create_rectangular_grid.c:4-440).  The large
@@ -35,7 +39,7 @@ class SW2Case:
     xyz: np.ndarray          # (V,3) float64
     tri: np.ndarray          # (T,3) int32
     seg: np.ndarray          # (S,2) int32
-    seg_kind: np.ndarray     # (S,) int32: 0 velocity, 1 depth
+    seg_kind: np.ndarray     # (S,) int32: 0 velocity, 1 depth, 2 discharge, 3 tailwater
     sol0: np.ndarray         # (3V,) float64 initial [h,u,v] per node
     dt: float
     nsteps: int
@@ -45,6 +49,9 @@ class SW2Case:
     inc_nonlin: float = 1e-6
     max_nonlin_it: int = 10
     gravity: float = GRAVITY
+    bc_conveyance: float = 1.0      # discharge string's conveyance (series 3 gives its series value)
+    bc_rough_height: float = 0.0    # equivalent roughness height of the boundary strings
+    # series ids: 0 depth, 1/2 velocity x/y, 3 discharge series value, 4 tailwater elevation
 
     @property
     def nnodes(self) -> int:
@@ -168,6 +175,38 @@ def flume_case(nsteps: int = 100, npx: int = 101, npy: int = 11) -> SW2Case:
     series = {0: _const_series(0.0, tf, 2.0), 1: _const_series(0.0, tf, 50.0 / (100.0 * 2.0)),
               2: _const_series(0.0, tf, 0.0)}
     return SW2Case("flume", xyz, tri, seg, kind, sol0, dt, nsteps, series)
+
+
+def bedshstr_drag_coef(depth: float, rough_height: float) -> float:
+    """The bed-shear drag coefficient c_f of a roughness height
+    (fr_bedshstr_drag_coef, src/friction/fr_bedshstr_drag_coef.c:18-42), for setting
+    boundary values on the host."""
+    depth = max(depth, 1e-8)
+    rough_height = max(rough_height, 1e-8)
+    depth_rh = 1.0 / 29.7 if rough_height > 29.7 * depth else depth / rough_height
+    bta = 29.7 * depth_rh
+    return 2.0 * ((0.4 * bta) / ((bta + 1) * (np.log(bta + 1) - 1) + 1)) ** 2
+
+
+def flume_structures_case(nsteps: int = 20, npx: int = 21, npy: int = 6, q_unit: float = 0.5,
+                          tail_depth: float = 2.0, rough_height: float = 0.05, conveyance: float = 1.0) -> SW2Case:
+    """The flume of ``flume_case`` driven by the structure conditions instead of the
+    velocity and depth ones: a discharge string on the x = 0 edge
+    (sw2_bc_discharge.c.bk: unit inflow q sqrt(2 g / c_f) h^(3/2) / conveyance, with its
+    series value q set so that the inflow is ``q_unit`` m^2/s at the initial 2 m depth)
+    and a tailwater string on the x = 1000 edge (sw2_bc_tailwater.c.bk: elevation
+    z_down + ``tail_depth``).  Boundary roughness height ``rough_height``."""
+    base = flume_case(nsteps=nsteps, npx=npx, npy=npy)
+    kind = np.where(base.seg_kind == 0, 2, 3).astype(np.int32)
+    z_down = float(base.xyz[base.seg[kind == 3][0, 0], 2])
+    c_f = bedshstr_drag_coef(2.0, rough_height)
+    q_series = q_unit * conveyance / (np.sqrt(2.0 * base.gravity / c_f) * 2.0 ** 1.5)
+    tf = base.dt * nsteps
+    series = dict(base.series)
+    series[3] = _const_series(0.0, tf, float(q_series))
+    series[4] = _const_series(0.0, tf, z_down + tail_depth)
+    return dataclasses.replace(base, name="flume_structures", seg_kind=kind, series=series,
+                               bc_conveyance=conveyance, bc_rough_height=rough_height)
 
 
 def still_beach_case(nsteps: int = 1440, npx: int = 16, npy: int = 6, nt: int = 1440) -> SW2Case:

@@ -89,6 +89,11 @@ class SW2Simulation:
         t_new = self.t + dt
         d, vx, vy = self.bc_values(t_new - dt, t_new)
         self.model.set_step(dt, d, vx, vy)
+        s = self.case.series
+        if 3 in s or 4 in s:    # discharge / tailwater segments
+            qs = series_step_average(*s[3], t_new - dt, t_new) if 3 in s else 0.0
+            tw = series_step_average(*s[4], t_new - dt, t_new) if 4 in s else 0.0
+            self.model.set_bc_structures(qs, self.case.bc_conveyance, self.case.bc_rough_height, tw)
         return t_new
 
     def _attempt(self, opts, dt):

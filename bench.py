@@ -53,9 +53,11 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["beach4M", "basin1M", "estuary16M"], default="beach4M",
-                   help="beach4M: the benchmark configuration; basin1M (fully wet tidal basin, dt 300 s) and "
-                        "estuary16M (partial wet/dry estuary, dt 180 s) measure the other GPU configurations")
+    p.add_argument("--workload", choices=["beach4M", "basin1M", "basin1M-hydro", "estuary16M"], default="beach4M",
+                   help="beach4M: the benchmark configuration; basin1M (fully wet tidal basin, dt 300 s), "
+                        "basin1M-hydro (the basin under a held-out inflow hydrograph, with the basin-trained "
+                        "learned guess) and estuary16M (partial wet/dry estuary, dt 180 s) measure the other "
+                        "GPU configurations")
     p.add_argument("--nx", type=int, default=2828)
     p.add_argument("--ny", type=int, default=707)
     p.add_argument("--krylov-tol", type=float, default=1e-6,
@@ -226,6 +228,9 @@ def run_ours(args, world, rank, local, dist):
     if args.workload == "basin1M":
         from adh_kraken_b200.mesh import basin_case
         case = basin_case(n=707, seed=2, nsteps=W + 2 * K + 8)
+    elif args.workload == "basin1M-hydro":
+        from adh_kraken_b200.mesh import basin_hydro_case
+        case = basin_hydro_case(48, n=707, nsteps=W + 2 * K + 8)     # a hydrograph the weights never saw
     elif args.workload == "estuary16M":
         from adh_kraken_b200.mesh import estuary_case
         case = estuary_case(nsteps=W + 2 * K + 8)
@@ -237,9 +242,10 @@ def run_ours(args, world, rank, local, dist):
     opts_fast = default_opts(krylov_precision=32, krylov_basis_precision=args.basis, **base)
     opts_plain = default_opts(krylov_precision=64, **base)
     guesser = None
-    if args.guess == "learned" and args.workload == "beach4M":
+    if args.guess == "learned" and args.workload in ("beach4M", "basin1M-hydro"):
         from adh_kraken_b200 import learned
-        guesser = learned.load_guesser(case, args.weights) if args.weights else learned.load_guesser(case)
+        default_w = learned.WEIGHTS if args.workload == "beach4M" else learned.BASIN_WEIGHTS
+        guesser = learned.load_guesser(case, args.weights or default_w)
     if guesser is not None:
         opts_fast.use_guess = 1
 

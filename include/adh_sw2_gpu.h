@@ -38,7 +38,9 @@ typedef struct {
     const double *xyz;      /* [3*nnodes] x, y, bed elevation z */
     const int *tri;         /* [3*ntri] counter-clockwise node ids */
     const int *seg;         /* [2*nseg] boundary segments; node order gives the outward normal */
-    const int *seg_kind;    /* [nseg] 0 = "NB VEL" (fe_sw2_bc_vel), 1 = "DEPTH" (fe_sw2_bc_h) */
+    const int *seg_kind;    /* [nseg] 0 = "NB VEL" (fe_sw2_bc_vel), 1 = "DEPTH" (fe_sw2_bc_h),
+                               2 = discharge (fe_sw2_bc_discharge, src/models/sw2/sw2_bc_discharge.c.bk:57),
+                               3 = tailwater (fe_sw2_bc_tailwater, src/models/sw2/sw2_bc_tailwater.c.bk:57) */
     const int *indptr;      /* optional [3*nnodes+1]: the caller's CSR, checked against ours; NULL to build */
     const int *cols;        /* optional [nnz] */
     double gravity;         /* sm->gravity, 9.8 by default */
@@ -132,6 +134,16 @@ int sw2g_get_sparsity(const sw2g_model *m, int *indptr, int *cols);
  * values of series 0 (depth) and 1/2 (velocity x/y) (sseries_setall_ts_valuesAVG,
  * src/structs/sseries/sseries.c:673). */
 int sw2g_set_step(sw2g_model *m, double dt, double tau_temporal, double bc_depth, double bc_vx, double bc_vy);
+/* The values of the discharge and tailwater segments (kinds 2 and 3) for the coming
+ * steps: the discharge string's series value (sseries_get_value of its ol_flow series,
+ * sw2_bc_discharge.c.bk:161), its conveyance (STR_VALUE.conveyance, sstr_value.h:63),
+ * the boundary strings' equivalent roughness height (FRICTION.eqrheight; the drag is
+ * fr_bedshstr_drag_coef's, zero for a height <= DBL_EPSILON as in fe_sw2_get_roughness,
+ * src/models/sw2/sw2_get_roughness.c:24) and the tailwater elevation (the series value of
+ * sw2_bc_tailwater.c.bk:154).  As in the reference, a discharge segment with zero drag
+ * divides by zero (the residual turns non-finite).  Defaults: 0, 1, 0, 0.  Non-finite
+ * values or a zero conveyance give SW2G_ERR_ARG. */
+int sw2g_set_bc_structures(sw2g_model *m, double q_series, double conveyance, double rough_height, double tail_elev);
 
 /* --- drop-in host-buffer entry points ------------------------------------ */
 /* fe_sw2_wdflag_legacy (src/models/sw2/sw2_wdflag_legacy.c:34): [ntri] flags 0/1/2 */

@@ -27,6 +27,7 @@ class _Model(C.Structure):
         ("gravity", C.c_double), ("dt", C.c_double), ("tau_temporal", C.c_double),
         ("bc_depth", C.c_double), ("bc_vx", C.c_double), ("bc_vy", C.c_double),
         ("wd_flag", _ip),
+        ("bc_qs", C.c_double), ("bc_convey", C.c_double), ("bc_rough", C.c_double), ("bc_tail", C.c_double),
     ]
 
 
@@ -111,6 +112,8 @@ class OracleModel:
         m.ndof, m.nnz, m.indptr, m.cols = 3 * V, nnz, _i(self.indptr), _i(self.cols)
         m.gravity, m.dt, m.tau_temporal = case.gravity, case.dt, float(tau_temporal)
         m.wd_flag = _i(self.wd_flag)
+        m.bc_convey = float(getattr(case, "bc_conveyance", 1.0))
+        m.bc_rough = float(getattr(case, "bc_rough_height", 0.0))
         self.m = m
         self.ndof, self.nnz = 3 * V, nnz
         self.set_bc_window(case.t0, case.t0 + case.dt)
@@ -125,6 +128,9 @@ class OracleModel:
 
     def set_bc_window(self, t1, t2):
         self.m.bc_depth, self.m.bc_vx, self.m.bc_vy = self.bc_values(t1, t2)
+        s = self.case.series
+        self.m.bc_qs = series_average(*s[3], t1, t2) if 3 in s else 0.0
+        self.m.bc_tail = series_average(*s[4], t1, t2) if 4 in s else 0.0
 
     # -- kernels
     def wd_flags(self, sol, sol_old):

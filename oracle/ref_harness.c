@@ -507,6 +507,89 @@ static void mode_rect(int argc, char **argv) {
     out_rec("grad_shp", 'd', grad, 6 * (int64_t)g.nelems2d);
 }
 
+/* Mode "bcx": the discharge and tailwater segment residuals of sw2_bc_discharge.c.bk and
+ * sw2_bc_tailwater.c.bk.  Those files are not part of the reference's build and do not
+ * compile against its live structures (the discharge file reads a NULL str_values, the
+ * tailwater file an older dof-map API), so their top-level steps are followed here line
+ * by line while every integral, the roughness law and the drag coefficient are the
+ * reference's own compiled functions (fe_sw2_1d_explicit_flow, fe_sw2_1d_wall_friction,
+ * fe_sw2_1d_implicit_flow, fe_sw2_1d_pressure in src/fe/fe_sw2_boundary_integrals.c,
+ * fe_sw2_get_roughness in src/models/sw2/sw2_get_roughness.c).  Input: int32 n, then n
+ * records of 21 doubles {kind, nx, ny, djac, dt, g, h0, h1, u0, v0, u1, v1, z0, q_series,
+ * conveyance, rough_height, tail_elev, perturbation, perturb_node, perturb_var (-1 none,
+ * 0 h, 1 u, 2 v), perturb_sign}; output record "seg_resid", 6 doubles per segment. */
+static void bcx_one(const double *in, double *out) {
+    int kind = (int)in[0];
+    SVECT2D nrml; nrml.x = in[1]; nrml.y = in[2];
+    double djac = in[3], dt = in[4], g = in[5];
+    double elem_head[2] = {in[6], in[7]};
+    SVECT2D elem_vel[2];
+    elem_vel[0].x = in[8]; elem_vel[0].y = in[9]; elem_vel[1].x = in[10]; elem_vel[1].y = in[11];
+    double z0 = in[12], qs = in[13], convey = in[14], rough = in[15], tail = in[16];
+    double perturbation = in[17];
+    int perturb_node = (int)in[18], perturb_var = (int)in[19], perturb_sign = (int)in[20];
+    int PRESSURE_FLAG = ON;
+    if (perturb_var == 0) elem_head[perturb_node] += perturb_sign * perturbation;
+    else if (perturb_var == 1) { elem_vel[perturb_node].x += perturb_sign * perturbation; PRESSURE_FLAG = OFF; }
+    else if (perturb_var == 2) { elem_vel[perturb_node].y += perturb_sign * perturbation; PRESSURE_FLAG = OFF; }
+    for (int i = 0; i < 6; i++) out[i] = 0.0;
+    SELEM_1D elem1d; memset(&elem1d, 0, sizeof elem1d);
+    STR_VALUE str; memset(&str, 0, sizeof str);
+    str.fterms.sav_flag = NO; str.fterms.urv_flag = NO; str.fterms.icethick = UNSET_FLT; str.fterms.eqrheight = rough;
+    SMODEL_SUPER mod; memset(&mod, 0, sizeof mod);
+    mod.str_values = &str;
+    if (kind == 2) {                       /* sw2_bc_discharge.c.bk:111-172 */
+        double u_tan = one_2 * (elem_vel[0].x + elem_vel[1].x) * nrml.y - one_2 * (elem_vel[0].y + elem_vel[1].y) * nrml.x;
+        double mag_utan = fabs(u_tan);
+        double u[2] = {elem_vel[0].x, elem_vel[1].x}, v[2] = {elem_vel[0].y, elem_vel[1].y};
+        double h_avg = one_2 * (elem_head[0] + elem_head[1]); if (h_avg < SMALL) h_avg = SMALL;
+        double roughness[2], resistance[2];
+        roughness[0] = fe_sw2_get_roughness(&mod, elem_head[0], 0.0, 0, UNUSED);
+        roughness[1] = fe_sw2_get_roughness(&mod, elem_head[1], 0.0, 0, UNUSED);
+        resistance[0] = one_2 * roughness[0] * mag_utan;
+        resistance[1] = one_2 * roughness[1] * mag_utan;
+        if (elem_head[0] < SMALL || elem_head[1] < SMALL) return;
+        double troughness[2], discharge[2], three_2 = 3.0 / 2.0;
+        troughness[0] = fe_sw2_get_roughness(&mod, elem_head[0], mag_utan, 0, UNUSED);
+        troughness[1] = fe_sw2_get_roughness(&mod, elem_head[1], mag_utan, 0, UNUSED);
+        double fact = -1.0 * qs * sqrt(2. * g / troughness[0]) / convey;
+        discharge[0] = fact * pow(elem_head[0], three_2);
+        fact = -1.0 * qs * sqrt(2. * g / troughness[1]) / convey;
+        discharge[1] = fact * pow(elem_head[0], three_2);
+        double elem_avg_discharge = one_2 * (discharge[0] + discharge[1]);
+        fe_sw2_1d_explicit_flow(out, elem1d, 0, nrml, djac, dt, elem_avg_discharge, h_avg, u, v, OFF, OFF);
+        fe_sw2_1d_wall_friction(out, elem1d, 0, nrml, djac, dt, u, v, resistance, OFF, OFF);
+    } else if (kind == 3) {                /* sw2_bc_tailwater.c.bk:152-170 */
+        double elem_depth[2];
+        elem_depth[0] = tail - z0;
+        elem_depth[1] = tail - z0;
+        if (elem_depth[0] < SMALL || elem_depth[1] < SMALL || elem_head[0] < SMALL || elem_head[1] < SMALL) return;
+        fe_sw2_1d_implicit_flow(out, elem1d, 0, nrml, djac, dt, elem_vel, elem_head, OFF, OFF);
+        if (PRESSURE_FLAG == ON) {
+            fe_sw2_1d_pressure(out, elem1d, 0, nrml, djac, dt, elem_depth, g, OFF, OFF);
+            fe_sw2_1d_pressure(out, elem1d, 0, nrml, djac, dt, elem_head, -g, OFF, OFF);
+        }
+    }
+}
+
+static int mode_bcx(const char *in_path, const char *out_path) {
+    FILE *f = fopen(in_path, "rb");
+    if (!f) { fprintf(stderr, "harness: cannot read %s\n", in_path); return 2; }
+    int32_t n = 0;
+    if (fread(&n, sizeof n, 1, f) != 1 || n < 0) { fclose(f); return 2; }
+    double *in = malloc(sizeof(double) * 21 * ((size_t)n + 1));
+    double *out = malloc(sizeof(double) * 6 * ((size_t)n + 1));
+    if (!in || !out || fread(in, sizeof(double), 21 * (size_t)n, f) != 21 * (size_t)n) { fclose(f); return 2; }
+    fclose(f);
+    for (int32_t k = 0; k < n; k++) bcx_one(in + 21 * (size_t)k, out + 6 * (size_t)k);
+    g_out = fopen(out_path, "wb");
+    if (!g_out) { fprintf(stderr, "harness: cannot write %s\n", out_path); return 2; }
+    out_rec("seg_resid", 'd', out, 6 * (int64_t)n);
+    fclose(g_out);
+    free(in); free(out);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc >= 4 && strcmp(argv[1], "geo") == 0) {
         if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
@@ -517,6 +600,12 @@ int main(int argc, char **argv) {
         mode_geo(argv);
         fclose(g_out);
         return 0;
+    }
+    if (argc >= 4 && strcmp(argv[1], "bcx") == 0) {
+        if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
+        debug_initialize();
+        sadh_def_init();
+        return mode_bcx(argv[2], argv[3]);
     }
     if (argc >= 4 && strcmp(argv[1], "rect") == 0) {
         if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }

@@ -111,3 +111,18 @@ def run_harness(mode, case=None, extra=(), sol=None, sol_old=None, sol_older=Non
         if r.returncode != 0:
             raise RuntimeError(f"harness {mode} failed ({r.returncode}): {r.stderr.decode()[-2000:]}")
         return read_records(opath)
+
+
+def run_bcx(records):
+    """Discharge / tailwater segment residuals computed by the reference's own boundary
+    integrals and roughness law (harness mode ``bcx``) for records of 21 doubles
+    {kind, nx, ny, djac, dt, g, h0, h1, u0, v0, u1, v1, z0, q_series, conveyance,
+    rough_height, tail_elev, perturbation, perturb_node, perturb_var, perturb_sign}."""
+    rec = np.ascontiguousarray(records, dtype="<f8").reshape(-1, 21)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "bcx.bin")
+        with open(p, "wb") as f:
+            f.write(struct.pack("<i", rec.shape[0]))
+            f.write(rec.tobytes())
+        out = run_harness("bcx", in_path=p)
+    return out["seg_resid"].reshape(-1, 6)

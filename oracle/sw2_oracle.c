@@ -554,7 +554,74 @@ static void pressure_1d(double *elem_rhs, v2 n, double djac, double dt, const do
     double t1 = dt * one_2 * g;
     for (int i = 0; i < 2; i++) { elem_rhs[i * 3 + 1] += t1 * n.x * r[i]; elem_rhs[i * 3 + 2] += t1 * n.y * r[i]; }
 }
-/* fe_sw2_bc_vel (src/models/sw2/sw2_bc_vel.c:58) and fe_sw2_bc_h (sw2_bc_h.c:57) */
+/* fr_bedshstr_drag_coef, src/friction/fr_bedshstr_drag_coef.c:18-42 */
+static double bedshstr_drag_coef(double depth, double rh) {
+    depth = depth > 1.E-8 ? depth : 1.E-8;
+    rh = rh > 1.E-8 ? rh : 1.E-8;
+    double depth_rh = (rh > 29.7 * depth) ? 1. / 29.7 : depth / rh;
+    double bta = 29.7 * depth_rh;
+    double phi = pow((.4 * bta) / ((bta + 1) * (log(bta + 1) - 1) + 1), 2.);
+    return 2. * phi;
+}
+/* fe_sw2_get_roughness (src/models/sw2/sw2_get_roughness.c:24-49), string without vegetation or ice */
+static double bc_roughness(double depth, double rh) { return rh > SMALL ? bedshstr_drag_coef(depth, rh) : 0.0; }
+/* integrate_line_phi / integrate_line_phi_f, src/fe/fe_integrals_1d.c:54,67 */
+static void line_phi(double djac, double c, double *q) { double t1 = one_2 * djac * c; q[0] += t1; q[1] += t1; }
+static void line_phi_f(double djac, double c, const double *f, double *q) {
+    double t1 = one_6 * djac * c;
+    q[0] += t1 * (2 * f[0] + f[1]);
+    q[1] += t1 * (f[0] + 2 * f[1]);
+}
+/* fe_sw2_1d_explicit_flow, src/fe/fe_sw2_boundary_integrals.c:56-82 */
+static void explicit_flow(double *elem_rhs, v2 n, double djac, double dt, double flux, double h_avg,
+                          const double *u, const double *v) {
+    double rc[2] = {0., 0.}, rx[2] = {0., 0.}, ry[2] = {0., 0.};
+    line_phi(djac, 1., rc);
+    if (flux < 0) {
+        double u_star = 0., v_star = 0.;
+        if (h_avg > 0) { u_star = flux * n.x / h_avg; v_star = flux * n.y / h_avg; }
+        line_phi(djac, u_star, rx);
+        line_phi(djac, v_star, ry);
+    } else {
+        line_phi_f(djac, 1., u, rx);
+        line_phi_f(djac, 1., v, ry);
+    }
+    double t1 = dt * flux;
+    for (int i = 0; i < 2; i++) {
+        elem_rhs[i * 3] += t1 * rc[i]; elem_rhs[i * 3 + 1] += t1 * rx[i]; elem_rhs[i * 3 + 2] += t1 * ry[i];
+    }
+}
+/* fe_sw2_1d_wall_friction, src/fe/fe_sw2_boundary_integrals.c:205-219 */
+static void wall_friction(double *elem_rhs, v2 n, double djac, double dt, const double *u, const double *v,
+                          const double *res) {
+    double rx[2] = {0., 0.}, ry[2] = {0., 0.};
+    line_phi_f(djac, fabs(n.y), u, rx);
+    line_phi_f(djac, fabs(n.x), v, ry);
+    for (int i = 0; i < 2; i++) { elem_rhs[i * 3 + 1] += dt * res[i] * rx[i]; elem_rhs[i * 3 + 2] += dt * res[i] * ry[i]; }
+}
+/* fe_sw2_bc_discharge (src/models/sw2/sw2_bc_discharge.c.bk:111-172): the discharge law
+ * -q sqrt(2 g / c_f) h^(3/2) / conveyance with the first node's head at both nodes, as an
+ * explicit flux, plus wall friction along the segment */
+static void discharge_resid(const sw2o_model *m, v2 n, double djac, double dt, const double *head, const v2 *vel,
+                            double *elem_rhs) {
+    double u_tan = one_2 * (vel[0].x + vel[1].x) * n.y - one_2 * (vel[0].y + vel[1].y) * n.x;
+    double mag_utan = fabs(u_tan);
+    double u[2] = {vel[0].x, vel[1].x}, v[2] = {vel[0].y, vel[1].y};
+    double h_avg = one_2 * (head[0] + head[1]);
+    if (h_avg < SMALL) h_avg = SMALL;
+    double res[2] = {one_2 * bc_roughness(head[0], m->bc_rough) * mag_utan,
+                     one_2 * bc_roughness(head[1], m->bc_rough) * mag_utan};
+    if (head[0] < SMALL || head[1] < SMALL) return;
+    double g = m->gravity;
+    double fact = -1.0 * m->bc_qs * sqrt(2. * g / bc_roughness(head[0], m->bc_rough)) / m->bc_convey;
+    double d0 = fact * pow(head[0], 1.5);
+    fact = -1.0 * m->bc_qs * sqrt(2. * g / bc_roughness(head[1], m->bc_rough)) / m->bc_convey;
+    double d1 = fact * pow(head[0], 1.5);
+    explicit_flow(elem_rhs, n, djac, dt, one_2 * (d0 + d1), h_avg, u, v);
+    wall_friction(elem_rhs, n, djac, dt, u, v, res);
+}
+/* fe_sw2_bc_vel (src/models/sw2/sw2_bc_vel.c:58), fe_sw2_bc_h (sw2_bc_h.c:57), and the
+ * discharge and tailwater conditions of sw2_bc_discharge.c.bk / sw2_bc_tailwater.c.bk */
 static void seg_resid(const sw2o_model *m, const double *sol, int k, double pert, int pnode, int pvar, int psign,
                       double *elem_rhs) {
     const int *nd = m->seg + 2 * k;
@@ -569,10 +636,21 @@ static void seg_resid(const sw2o_model *m, const double *sol, int k, double pert
     if (m->seg_kind[k] == 0) {
         vel[0].x = m->bc_vx; vel[0].y = m->bc_vy; vel[1].x = m->bc_vx; vel[1].y = m->bc_vy;
         implicit_flow(elem_rhs, n, djac, dt, vel, head);
-    } else {
+    } else if (m->seg_kind[k] == 1) {
         double dep[2] = {m->bc_depth, m->bc_depth};
         if (dep[0] < SMALL || dep[1] < SMALL || head[0] < SMALL || head[1] < SMALL) return;
         implicit_flow(elem_rhs, n, djac, dt, vel, dep);
+        if (pressure) {
+            pressure_1d(elem_rhs, n, djac, dt, dep, m->gravity);
+            pressure_1d(elem_rhs, n, djac, dt, head, -m->gravity);
+        }
+    } else if (m->seg_kind[k] == 2) {
+        discharge_resid(m, n, djac, dt, head, vel, elem_rhs);
+    } else {   /* sw2_bc_tailwater.c.bk:152-170: depth below the elevation at the first node, at both */
+        double z0 = m->xyz[3 * nd[0] + 2];
+        double dep[2] = {m->bc_tail - z0, m->bc_tail - z0};
+        if (dep[0] < SMALL || dep[1] < SMALL || head[0] < SMALL || head[1] < SMALL) return;
+        implicit_flow(elem_rhs, n, djac, dt, vel, head);
         if (pressure) {
             pressure_1d(elem_rhs, n, djac, dt, dep, m->gravity);
             pressure_1d(elem_rhs, n, djac, dt, head, -m->gravity);

@@ -22,7 +22,8 @@ typedef struct {
     const double *xyz;       /* 3*nnodes: x, y, bed z */
     const int *tri;          /* 3*ntri, counter-clockwise */
     const int *seg;          /* 2*nseg, node order gives the outward normal */
-    const int *seg_kind;     /* nseg: 0 = NB VEL (fe_sw2_bc_vel), 1 = DEPTH (fe_sw2_bc_h) */
+    const int *seg_kind;     /* nseg: 0 = NB VEL (fe_sw2_bc_vel), 1 = DEPTH (fe_sw2_bc_h),
+                                2 = discharge (sw2_bc_discharge.c.bk), 3 = tailwater (sw2_bc_tailwater.c.bk) */
     const double *tri_djac;  /* ntri: element area */
     const double *tri_grad;  /* 6*ntri: grad phi_a (x,y) for a = 0..2 */
     const double *seg_djac;  /* nseg: segment length */
@@ -35,6 +36,10 @@ typedef struct {
     double tau_temporal;     /* alpha of the 3-level scheme, 0 = backward Euler */
     double bc_depth, bc_vx, bc_vy; /* step-averaged series values (ids 0, 1, 2) */
     int *wd_flag;            /* ntri, written by sw2o_wd_flags */
+    double bc_qs;            /* discharge string's series value */
+    double bc_convey;        /* discharge string's conveyance */
+    double bc_rough;         /* boundary strings' equivalent roughness height */
+    double bc_tail;          /* tailwater elevation */
 } sw2o_model;
 
 /* geometry: selem2d_get_triangle_linear_djac_nrml_gradPhi (src/structs/selem/selem_2d.c:270-350),
