@@ -452,3 +452,43 @@ class RankNewton:
             sol[mask_own == 1] = dirichlet_own[mask_own == 1]
         return sol, {"newton_its": it, "krylov_its": kry, "resid_max": rmax, "ok": success,
                      "linesearch_cuts": cuts_total}
+
+
+class DeviceRankModel:
+    """The device model (``capi.SW2Model``, the CUDA element and assembly kernels) as
+    RankNewton's element evaluator for one rank's halo sub-mesh.  Like fe_sw2_init
+    (src/models/sw2/fe_sw2_init.c), ``wd_flags`` fixes the wet/dry flags at the start of
+    a Newton solve and every residual and Jacobian of that solve uses them
+    (``sw2g_assemble_residual_wd`` / ``sw2g_assemble_jacobian_wd``)."""
+
+    def __init__(self, sub_case):
+        from .capi import SW2Model
+        self.case = sub_case
+        self.model = SW2Model(sub_case)
+        self.indptr = self.model.sparsity()[0]
+        self._wd = None
+        self.set_bc_window(sub_case.t0, sub_case.t0 + sub_case.dt)
+
+    def set_bc_window(self, t1: float, t2: float) -> None:
+        """The step's dt and series averages over [t1, t2] (advance_time's series update)."""
+        from .timeloop import series_step_average
+        s = self.case.series
+        vals = [series_step_average(*s[k], t1, t2) if k in s else 0.0 for k in (0, 1, 2)]
+        self.model.set_step(t2 - t1, *vals)
+        if 3 in s or 4 in s:
+            qs = series_step_average(*s[3], t1, t2) if 3 in s else 0.0
+            tw = series_step_average(*s[4], t1, t2) if 4 in s else 0.0
+            self.model.set_bc_structures(qs, self.case.bc_conveyance, self.case.bc_rough_height, tw)
+
+    def wd_flags(self, sol, sol_old):
+        self._wd = self.model.wd_flags(sol, sol_old)
+        return self._wd.copy()
+
+    def residual(self, sol, sol_old, sol_older):
+        return self.model.residual_wd(sol, sol_old, sol_older, self._wd)
+
+    def jacobian(self, sol, sol_old, sol_older):
+        return self.model.jacobian_wd(sol, sol_old, sol_older, self._wd)
+
+    def close(self) -> None:
+        self.model.close()
