@@ -73,6 +73,13 @@ class SW2Simulation:
         self.model.load_state(sol0, sol0, sol0)
         self.history = []        # every Newton solve tried, failed ones included
         self.nsteps_done = 0     # successful steps (what a checkpoint counts)
+        # advance(): after an interval needed a cut, the next intervals start at the reduced
+        # step (the reference keeps a cut dt too: tc_scale writes sm->ts->dt and nothing
+        # restores it); after keep_reduced_dt such intervals the step grows by 1/DT_REDUCE_FACTOR
+        # toward the case's dt.  0 turns the carry-over off.
+        self.keep_reduced_dt = 4
+        self.dt_hold = None      # the reduced step carried over, None = the case's dt
+        self.hold_count = 0      # intervals completed at dt_hold
         self.mass_log = None
         self.log = None     # a writable text stream: one JSON line per step (set_log)
 
@@ -166,22 +173,37 @@ class SW2Simulation:
         reductions (success 0, the state and the clock at the last good substep).  With
         the relative Newton test, the shorter steps keep the tolerance of the interval's
         first attempt (sw2g_newton_opts.tol_nonlin_min).
+        After an interval that needed a cut, the next ``keep_reduced_dt`` intervals start
+        at the reduced step (with the interval's tolerance), then the step grows back by
+        1/DT_REDUCE_FACTOR per such run of intervals.
         ``before_attempt(sim, dt)``, when given, runs before every Newton solve (e.g.
         to set an initial guess for a step of that dt).  Failed attempts are undone before anything else runs:
         the clock never moves for them and the mass log never sees them."""
         target = self.t + self.case.dt
         dt, cuts, subs, failed = self.case.dt, 0, [], []
         o_cur = opts or self.opts
+        rel = getattr(o_cur, "tol_nonlin_rel", 0)
+        held = self.keep_reduced_dt > 0 and self.dt_hold is not None and self.dt_hold < self.case.dt
+        if held:
+            dt = self.dt_hold
+            if rel > 0:
+                # R(sol_old) scales with the step's length (sol = sol_old makes the temporal
+                # terms vanish), so rel x dt/h keeps the tolerance of the whole interval
+                o_cur = type(o_cur).from_buffer_copy(o_cur)
+                o_cur.tol_nonlin_rel = rel * self.case.dt / dt
+        first = True
         while self.t + NOT_QUITE_SMALL * self.case.dt < target:
             h = min(dt, target - self.t)
             if before_attempt is not None:
                 before_attempt(self, h)
             st, t_new = self._attempt(o_cur, h)
-            if cuts == 0 and not st["success"] and st.get("tol_used") and getattr(o_cur, "tol_nonlin_rel", 0) > 0:
+            if first and rel > 0 and st.get("tol_used") and (held or not st["success"]):
                 # the shorter steps keep the interval's tolerance: the residual at the start of a
                 # short step shrinks with its dt, the attainable accuracy does not
                 o_cur = type(o_cur).from_buffer_copy(o_cur)
                 o_cur.tol_nonlin_min = float(st["tol_used"])
+                o_cur.tol_nonlin_rel = rel
+            first = False
             if st["success"]:
                 self._record(st, t_new, h, moved=True)
                 subs.append(st)
@@ -194,7 +216,16 @@ class SW2Simulation:
                 break
             dt = h * DT_REDUCE_FACTOR
         ok = cuts <= max_cuts
-        out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts,
+        if ok and self.keep_reduced_dt > 0:
+            if cuts > 0:
+                self.dt_hold, self.hold_count = dt, 0
+            elif held:
+                self.hold_count += 1
+                if self.hold_count >= self.keep_reduced_dt:
+                    grown = dt / DT_REDUCE_FACTOR
+                    self.dt_hold = None if grown >= self.case.dt * (1 - NOT_QUITE_SMALL) else grown
+                    self.hold_count = 0
+        out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts, "step_start": dt if held else self.case.dt,
                "newton_its": sum(s["newton_its"] for s in subs + failed),
                "krylov_its": sum(s["krylov_its"] for s in subs + failed),
                "linear_unconverged": sum(s.get("linear_unconverged", 0) for s in subs + failed)}
@@ -249,7 +280,8 @@ class SW2Simulation:
             extra = {"mass_density": self.density, "mass0": self.mass0, "mass_inflow_total": self.inflow_total,
                      "mass_log": np.asarray(self.mass_log, dtype=np.float64).reshape(-1, 3)}
         np.savez(path, sol=sol, sol_old=sol_old, sol_older=sol_older, bc_mask=bc_mask, t=self.t,
-                 dt=self.case.dt, steps=self.nsteps_done, **extra)
+                 dt=self.case.dt, steps=self.nsteps_done,
+                 dt_hold=-1.0 if self.dt_hold is None else self.dt_hold, hold_count=self.hold_count, **extra)
 
     def restore(self, path: str) -> None:
         z = np.load(path)
@@ -258,6 +290,9 @@ class SW2Simulation:
         self.model.load_state(z["sol"], z["sol_old"], z["sol_older"], bc_mask=z["bc_mask"])
         self.t = float(z["t"])
         self.nsteps_done = int(z["steps"])
+        if "dt_hold" in z:
+            self.dt_hold = None if float(z["dt_hold"]) < 0 else float(z["dt_hold"])
+            self.hold_count = int(z["hold_count"])
         if "mass0" in z:
             self.density = float(z["mass_density"])
             self.mass0 = float(z["mass0"])

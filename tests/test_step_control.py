@@ -80,3 +80,46 @@ def test_mass_bookkeeping_counts_successful_steps_only():
     assert mb["steps"] == 4
     assert mb["inflow"] == pytest.approx(2.0 * 2.0 * case.dt)
     assert mb["error"] == pytest.approx(0.0, abs=1e-9)
+
+
+def test_advance_keeps_a_reduced_dt_then_grows_it_back():
+    """After a cut, the next keep_reduced_dt intervals start at the reduced step (no
+    failed full-dt attempt), then the full dt is tried again; keep_reduced_dt = 0 tries
+    it every interval."""
+    case = flume_case(nsteps=8, npx=5, npy=3)
+    q = case.dt * DT_REDUCE_FACTOR
+    fake = FakeModel(dt_ok=q)
+    sim = SW2Simulation(case, model=fake)
+    cuts = [sim.advance()["dt_cuts"] for _ in range(7)]
+    assert cuts == [1, 0, 0, 0, 0, 1, 0]
+    assert fake.calls == ([case.dt] + [q] * 4) + [q] * 16 + ([case.dt] + [q] * 4) + [q] * 4
+    assert sim.t == pytest.approx(case.t0 + 7 * case.dt)
+    fake0 = FakeModel(dt_ok=q)
+    sim0 = SW2Simulation(case, model=fake0)
+    sim0.keep_reduced_dt = 0
+    assert [sim0.advance()["dt_cuts"] for _ in range(3)] == [1, 1, 1]
+
+
+def test_held_step_keeps_the_interval_tolerance():
+    """A held step h starts with tol_nonlin_rel x dt / h (R(sol_old) scales with the step's
+    length), and its later substeps keep the first one's tolerance as the floor."""
+    from adh_kraken_b200.capi import default_opts
+    case = flume_case(nsteps=4, npx=5, npy=3)
+    seen = []
+
+    class Recording(FakeModel):
+        def step(self, opts=None):
+            seen.append((self.dt, opts.tol_nonlin_rel, opts.tol_nonlin_min))
+            st = super().step(opts)
+            st["tol_used"] = 1e-8 * (self.dt / case.dt) * opts.tol_nonlin_rel / 1e-8 * 3.0
+            return st
+
+    fake = Recording(dt_ok=case.dt * DT_REDUCE_FACTOR)
+    sim = SW2Simulation(case, model=fake, opts=default_opts(tol_nonlin_rel=1e-8))
+    sim.advance()
+    seen.clear()
+    sim.advance()
+    q = case.dt * DT_REDUCE_FACTOR
+    assert seen[0] == (q, pytest.approx(1e-8 / DT_REDUCE_FACTOR), 0.0)
+    first_tol = 1e-8 * DT_REDUCE_FACTOR * (1e-8 / DT_REDUCE_FACTOR) / 1e-8 * 3.0
+    assert all(s[1] == pytest.approx(1e-8) and s[2] == pytest.approx(first_tol) for s in seen[1:])
