@@ -51,6 +51,49 @@ __device__ __forceinline__ bool gm_last_block(const GmresDev& G) {
     return is_last;
 }
 
+// 16-byte loads and stores of basis entries (4 floats or 2 doubles); the basis stride is a
+// multiple of 4 entries, so every vector starts on a 16-byte boundary.
+template <class VT> struct Quad { static constexpr int N = 16 / sizeof(VT); };
+__device__ __forceinline__ void ld16(const float* p, float (&o)[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+}
+__device__ __forceinline__ void ld16(const double* p, double (&o)[2]) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = t.x; o[1] = t.y;
+}
+__device__ __forceinline__ void ld16_rw(const float* p, float (&o)[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+}
+__device__ __forceinline__ void ld16_rw(const double* p, double (&o)[2]) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    o[0] = t.x; o[1] = t.y;
+}
+__device__ __forceinline__ void st16(float* p, const float (&o)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void st16(double* p, const double (&o)[2]) {
+    *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+}
+
+// In the last block, the sum of column col of the blocks' partials by all its threads
+// (each thread a fixed stride of blocks, then the warp and block trees): the result in
+// thread 0.  Every thread of the block calls it.
+__device__ __forceinline__ double gm_sum_partials(const GmresDev& G, int col) {
+    __shared__ double red[8];
+    double t = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += __ldcg(G.partial + b * (kGmM + 1) + col);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    double s = 0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += red[k];
+    return s;
+}
+
 // beta = ||r||_2 ; g = beta e_0 ; target = rtol * beta ; columns = 0
 template <class VT>
 __global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ r, const double* __restrict__ rw,
@@ -70,10 +113,10 @@ __global__ void __launch_bounds__(256) k_gm_start(int n, const VT* __restrict__ 
         for (int k = 0; k < 8; k++) t += sh[k];
         G.partial[blockIdx.x * (kGmM + 1)] = t;
     }
-    if (gm_last_block(G) && threadIdx.x == 0) {
-        double t = 0;
-        for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1));
-        const double beta = sqrt(t);
+    if (!gm_last_block(G)) return;
+    const double tsum = gm_sum_partials(G, 0);
+    if (threadIdx.x == 0) {
+        const double beta = sqrt(tsum);
         G.scal[0] = beta;
         G.scal[1] = G.scal[3] * beta;       // stopping target on |g_{j+1}|
         G.scal[2] = beta;
@@ -117,7 +160,24 @@ __global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __rest
     double acc[kDotGroup];
 #pragma unroll
     for (int k = 0; k < kDotGroup; k++) acc[k] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    constexpr int NQ = Quad<VT>::N;
+    const int nq = n / NQ;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)q * NQ;
+        VT wq[NQ];
+        ld16_rw(w + i, wq);
+        VT x[kDotGroup][NQ];
+#pragma unroll
+        for (int k = 0; k < kDotGroup; k++)
+            if (k0 + k < nv) ld16(Vb + (size_t)(k0 + k) * ld + i, x[k]);
+#pragma unroll
+        for (int k = 0; k < kDotGroup; k++)
+            if (k0 + k < nv) {
+#pragma unroll
+                for (int c = 0; c < NQ; c++) acc[k] += (double)x[k][c] * (double)wq[c];
+            }
+    }
+    for (int i = nq * NQ + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double wi = w[i];
 #pragma unroll
         for (int k = 0; k < kDotGroup; k++)
@@ -139,11 +199,13 @@ __global__ void __launch_bounds__(256) k_gm_dots(int n, int nv, const VT* __rest
         for (int w8 = 0; w8 < 8; w8++) t += sh[w8][threadIdx.x];
         G.partial[blockIdx.x * (kGmM + 1) + k0 + threadIdx.x] = t;
     }
-    if (gm_last_block(G)) {
-        if (threadIdx.x < nv) {
+    if (gm_last_block(G)) {   // warp w sums columns w, w + 8, ...; its lanes stride over the blocks
+        for (int c = warp; c < nv; c += (int)(blockDim.x >> 5)) {
             double t = 0;
-            for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1) + threadIdx.x);
-            dst[threadIdx.x] = t;
+            for (int b = lane; b < (int)gridDim.x; b += 32) t += __ldcg(G.partial + b * (kGmM + 1) + c);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) dst[c] = t;
         }
     }
 }
@@ -184,17 +246,44 @@ __global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ 
     __syncthreads();
     VT* w = Vb + (size_t)(j + 1) * ld;
     double ss = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double v = w[i];
+    constexpr int NQ = Quad<VT>::N;
+    const int nq = n / NQ;
+    // NQ consecutive entries per thread, eight 16-byte basis loads in flight, then the
+    // updates of each entry in basis order (the same arithmetic per entry as one at a time)
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)q * NQ;
+        VT wq[NQ];
+        ld16_rw(w + i, wq);
+        double v[NQ];
+#pragma unroll
+        for (int c = 0; c < NQ; c++) v[c] = wq[c];
         int k = 0;
-        for (; k + 8 <= j + 1; k += 8) {   // eight basis loads in flight, then the updates in order
-            double x[8];
+        for (; k + 8 <= j + 1; k += 8) {
+            VT x[8][NQ];
 #pragma unroll
-            for (int u = 0; u < 8; u++) x[u] = (double)Vb[(size_t)(k + u) * ld + i];
+            for (int u = 0; u < 8; u++) ld16(Vb + (size_t)(k + u) * ld + i, x[u]);
 #pragma unroll
-            for (int u = 0; u < 8; u++) v -= h[k + u] * x[u];
+            for (int u = 0; u < 8; u++)
+#pragma unroll
+                for (int c = 0; c < NQ; c++) v[c] -= h[k + u] * (double)x[u][c];
         }
-        for (; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
+        for (; k <= j; k++) {
+            VT x[NQ];
+            ld16(Vb + (size_t)k * ld + i, x);
+#pragma unroll
+            for (int c = 0; c < NQ; c++) v[c] -= h[k] * (double)x[c];
+        }
+        VT o[NQ];
+#pragma unroll
+        for (int c = 0; c < NQ; c++) {
+            o[c] = (VT)v[c];
+            ss += (double)o[c] * (double)o[c];
+        }
+        st16(w + i, o);
+    }
+    for (int i = nq * NQ + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = w[i];
+        for (int k = 0; k <= j; k++) v -= h[k] * (double)Vb[(size_t)k * ld + i];
         const VT vv = (VT)v;
         w[i] = vv;
         ss += (double)vv * (double)vv;
@@ -208,10 +297,10 @@ __global__ void __launch_bounds__(256) k_gm_orth(int n, int j, VT* __restrict__ 
         for (int k = 0; k < 8; k++) t += sh[k];
         G.partial[blockIdx.x * (kGmM + 1)] = t;
     }
-    if (gm_last_block(G) && threadIdx.x == 0) {
-        double t = 0;
-        for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(G.partial + b * (kGmM + 1));
-        const double hn = sqrt(t);
+    if (!gm_last_block(G)) return;
+    const double tsum = gm_sum_partials(G, 0);
+    if (threadIdx.x == 0) {
+        const double hn = sqrt(tsum);
         double* col = G.H + j * (kGmM + 1);
         if (SECOND)
             for (int k = 0; k <= j; k++) col[k] += G.H2[k];

@@ -89,8 +89,8 @@ struct sw2g_model {
     bool amg_ready = false;
     // restarted GMRES (allocated on first use)
     GmresDev gm{};
-    double* gm_V64 = nullptr;            // [cap+1][n] Krylov basis
-    float* gm_V32 = nullptr;             // [cap+1][n] FP32 Krylov basis (krylov_basis_precision 32)
+    double* gm_V64 = nullptr;            // [cap+1][gm_ld(n)] Krylov basis
+    float* gm_V32 = nullptr;             // [cap+1][gm_ld(n)] FP32 Krylov basis (krylov_basis_precision 32)
     int gm_cap64 = 0, gm_cap32 = 0;      // restart length the bases were allocated for
     cudaGraphExec_t gm_graph_b32 = nullptr;
     int gm_m64 = 0, gm_m32 = 0, gm_mb32 = 0;   // restart length each cycle graph was built for
@@ -964,13 +964,17 @@ static int alloc_gmres(sw2g_model* m) {
     return SW2G_OK;
 }
 
+// Stride of the Krylov basis: n rounded up to 4 entries, so that every basis vector
+// starts on a 16-byte boundary (the Gram-Schmidt kernels read 16 bytes per load)
+static size_t gm_ld(int n) { return ((size_t)n + 3) & ~(size_t)3; }
+
 // Krylov basis of mres + 1 vectors, grown when a longer restart is asked for
 template <class T>
 static int gmres_basis(sw2g_model* m, T** V, int* cap, int mres) {
     if (*V && *cap >= mres) return SW2G_OK;
     CK(cudaStreamSynchronize(m->st));
     dfree(m, V);
-    TRY(dalloc(m, V, (size_t)(mres + 1) * m->n));
+    TRY(dalloc(m, V, (size_t)(mres + 1) * gm_ld(m->n)));
     *cap = mres;
     return SW2G_OK;
 }
@@ -992,7 +996,7 @@ static int gmres_graph32(sw2g_model* m, cudaGraphExec_t* graph, int* built_m, in
     op.vals = m->f_vals;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-    gmres_cycle<float>(m->B, op, m->f_vals, m->gm_V32, (size_t)m->n, m->f_z, m->f_b, m->f_x, m->gm_rw, m->gm, m->st,
+    gmres_cycle<float>(m->B, op, m->f_vals, m->gm_V32, gm_ld(m->n), m->f_z, m->f_b, m->f_x, m->gm_rw, m->gm, m->st,
                        mres, gm_reorth());
     cudaError_t e1 = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
@@ -1015,7 +1019,7 @@ static int gmres_graph(sw2g_model* m, cudaGraphExec_t* graph, int* built_m, bool
     if (mixed) { op.mixed = true; op.vals32 = m->f_vals; op.lu32 = m->f_lu; op.dinv32 = m->f_inv; op.tmp32 = m->f_z; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-    gmres_cycle<double>(m->B, op, m->d_vals, m->gm_V64, (size_t)m->n, m->k_z, m->d_t64, m->k_xi, m->gm_rw, m->gm,
+    gmres_cycle<double>(m->B, op, m->d_vals, m->gm_V64, gm_ld(m->n), m->k_z, m->d_t64, m->k_xi, m->gm_rw, m->gm,
                         m->st, mres, gm_reorth());
     cudaError_t e1 = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
