@@ -20,7 +20,7 @@ _ip = C.POINTER(C.c_int)
 # every symbol declared in include/adh_sw2_gpu.h
 EXPORTED = [
     "sw2g_create", "sw2g_destroy", "sw2g_last_error", "sw2g_default_opts", "sw2g_sizes", "sw2g_get_sparsity",
-    "sw2g_set_step", "sw2g_set_bc_structures", "sw2g_wd_flags", "sw2g_elem_resid", "sw2g_elem_jac", "sw2g_assemble_residual",
+    "sw2g_set_step", "sw2g_set_bc_structures", "sw2g_set_bc_flux", "sw2g_wd_flags", "sw2g_elem_resid", "sw2g_elem_jac", "sw2g_assemble_residual",
     "sw2g_assemble_jacobian", "sw2g_prepare_system", "sw2g_solve_linear_sys_bcgstab", "sw2g_fe_newton",
     "sw2g_load_state", "sw2g_store_state", "sw2g_set_guess", "sw2g_step", "sw2g_device_state", "sw2g_stream",
     "sw2g_set_profiling", "sw2g_get_profile", "sw2g_reset_profile", "sw2g_time_kernel",
@@ -167,6 +167,10 @@ class SW2Model:
         """Values of the discharge (kind 2) and tailwater (kind 3) segments."""
         self._check(lib().sw2g_set_bc_structures(self.h, C.c_double(q_series), C.c_double(conveyance),
                                                  C.c_double(rough_height), C.c_double(tail_elev)))
+
+    def set_bc_flux(self, flux_series):
+        """Series value of the flux segments (kind 5)."""
+        self._check(lib().sw2g_set_bc_flux(self.h, C.c_double(flux_series)))
 
     def set_step(self, dt, bc_depth, bc_vx, bc_vy, tau_temporal=0.0):
         self._check(lib().sw2g_set_step(self.h, C.c_double(dt), C.c_double(tau_temporal), C.c_double(bc_depth),

@@ -217,7 +217,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
     if ((long)(T + S) * 9 >= (1L << 31) || 3L * V >= (1L << 31)) { g_err = "sw2g_create: mesh too large for 32-bit maps"; return SW2G_ERR_ARG; }
     for (long i = 0; i < 3L * T; i++) if (mesh->tri[i] < 0 || mesh->tri[i] >= V) { g_err = "sw2g_create: triangle node id out of range"; return SW2G_ERR_MESH; }
     for (long i = 0; i < 2L * S; i++) if (mesh->seg[i] < 0 || mesh->seg[i] >= V) { g_err = "sw2g_create: segment node id out of range"; return SW2G_ERR_MESH; }
-    for (int i = 0; i < S; i++) if (mesh->seg_kind[i] < 0 || mesh->seg_kind[i] > 3) { g_err = "sw2g_create: segment kind not in 0..3"; return SW2G_ERR_ARG; }
+    for (int i = 0; i < S; i++) if (mesh->seg_kind[i] < 0 || mesh->seg_kind[i] > 5) { g_err = "sw2g_create: segment kind not in 0..5"; return SW2G_ERR_ARG; }
     sw2g_model* m = new sw2g_model();
     m->V = V; m->T = T; m->S = S; m->Etot = T + S; m->n = 3 * V;
     if (cudaGetDevice(&m->device) != cudaSuccess) { g_err = "sw2g_create: no current CUDA device"; delete m; return SW2G_ERR_CUDA; }
@@ -407,7 +407,7 @@ extern "C" int sw2g_create(const sw2g_mesh* mesh, void* cuda_stream, sw2g_model*
                     m->d_seg, m->d_snx, m->d_sny, m->d_sdjac, m->d_skind, m->d_sz0};
     m->A = AssemblyMaps{m->nslots, m->d_rptr, m->d_rmap, m->d_jptr, m->d_jmap, m->d_boff, m->d_blen};
     m->B = BlockCSR{V, m->n, m->nnz, m->d_indptr, m->d_cols, m->d_bptr, m->d_bcol, m->d_diag};
-    m->P = StepParams{1.0, 0.0, mesh->gravity, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0};
+    m->P = StepParams{1.0, 0.0, mesh->gravity, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0};
     CK(cudaStreamSynchronize(m->st));
     *out = m;
     return SW2G_OK;
@@ -473,6 +473,12 @@ extern "C" int sw2g_set_bc_structures(sw2g_model* m, double q_series, double con
     }
     if (conveyance == 0.0) { g_err = "sw2g_set_bc_structures: zero conveyance"; return SW2G_ERR_ARG; }
     m->P.bc_qs = q_series; m->P.bc_convey = conveyance; m->P.bc_rough = rough_height; m->P.bc_tail = tail_elev;
+    return SW2G_OK;
+}
+extern "C" int sw2g_set_bc_flux(sw2g_model* m, double flux_series) {
+    if (!m) { g_err = "sw2g_set_bc_flux: null model"; return SW2G_ERR_ARG; }
+    if (!std::isfinite(flux_series)) { g_err = "sw2g_set_bc_flux: non-finite value"; return SW2G_ERR_ARG; }
+    m->P.bc_flux = flux_series;
     return SW2G_OK;
 }
 extern "C" void* sw2g_stream(sw2g_model* m) { return m ? (void*)m->st : nullptr; }

@@ -24,7 +24,7 @@ struct MeshView {
     const double* snx;    // [nseg] outward normal
     const double* sny;
     const double* sdjac;  // [nseg] length
-    const int* skind;     // [nseg] 0 velocity, 1 depth, 2 discharge, 3 tailwater
+    const int* skind;     // [nseg] 0 velocity, 1 depth, 2 discharge, 3 tailwater, 4 outflow, 5 flux
     const double* sz0;    // [nseg] bed elevation of the segment's first node
 };
 
@@ -34,6 +34,7 @@ struct StepParams {
     double grav;
     double bc_depth, bc_vx, bc_vy;   // step-averaged series 0, 1, 2
     double bc_qs, bc_convey, bc_rough, bc_tail;   // discharge series value, conveyance, roughness height, tailwater elevation
+    double bc_flux;                               // flux string's series value
 };
 
 // Deterministic assembly maps (built once from the bit-exact CSR):

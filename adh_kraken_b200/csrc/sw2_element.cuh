@@ -488,7 +488,7 @@ struct SegData {
     V2 n; double djac;
     double h[2]; V2 vel[2];
     double z0;  // bed elevation of the segment's first node
-    int kind;   // 0 velocity (fe_sw2_bc_vel), 1 depth (fe_sw2_bc_h), 2 discharge, 3 tailwater
+    int kind;   // 0 velocity (fe_sw2_bc_vel), 1 depth (fe_sw2_bc_h), 2 discharge, 3 tailwater, 4 outflow, 5 flux
 };
 
 // The boundary values of one step, shared by every segment of a kind.
@@ -498,6 +498,7 @@ struct SegBC {
     double conveyance;      // discharge string's conveyance (sstr_value.h:63)
     double rough_height;    // equivalent roughness height of the boundary strings (FRICTION.eqrheight)
     double tail_elev;       // tailwater elevation series value (sw2_bc_tailwater.c.bk:154)
+    double flux_series;     // flux string's series value (sw2_bc_flux.c.bk:152)
 };
 
 // fr_bedshstr_drag_coef, src/friction/fr_bedshstr_drag_coef.c:18-42
@@ -622,6 +623,13 @@ __device__ __forceinline__ void seg_resid(const SegData& S, double dt, double gr
         double d1 = fact * pow(S.h[0], 1.5);
         explicit_flow(r, S.n, S.djac, dt, SW2_ONE_2 * (d0 + d1), h_avg, u, v);
         wall_friction(r, S.n, S.djac, dt, u, v, res);
+    } else if (S.kind == 4) {   // sw2_bc_outflow.c.bk:144: implicit flow with the computed depth and velocity
+        implicit_flow(r, S.n, S.djac, dt, S.vel, S.h);
+    } else if (S.kind == 5) {   // sw2_bc_flux.c.bk:151-153: the series value as a unit inflow
+        double u[2] = {S.vel[0].x, S.vel[1].x}, v[2] = {S.vel[0].y, S.vel[1].y};
+        double h_avg = SW2_ONE_2 * (S.h[0] + S.h[1]);
+        if (h_avg < SW2_SMALL) h_avg = SW2_SMALL;
+        explicit_flow(r, S.n, S.djac, dt, -1.0 * B.flux_series, h_avg, u, v);
     } else {                    // kind 3: sw2_bc_tailwater.c.bk:152-170
         // depth below the tailwater elevation at the first node, used at both nodes (.bk:155-156)
         double dep[2] = {B.tail_elev - S.z0, B.tail_elev - S.z0};

@@ -39,7 +39,7 @@ __device__ __forceinline__ void load_tri(const MeshView& M, const double* __rest
 }
 
 __device__ __forceinline__ SegBC seg_bc(const StepParams& P) {
-    return SegBC{P.bc_depth, P.bc_vx, P.bc_vy, P.bc_qs, P.bc_convey, P.bc_rough, P.bc_tail};
+    return SegBC{P.bc_depth, P.bc_vx, P.bc_vy, P.bc_qs, P.bc_convey, P.bc_rough, P.bc_tail, P.bc_flux};
 }
 
 __device__ __forceinline__ void load_seg(const MeshView& M, const double* __restrict__ sol, int s, SegData& S) {

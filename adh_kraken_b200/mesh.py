@@ -10,12 +10,13 @@ conventions:
 * ``seg_kind`` 0 for a weak velocity boundary ("NB VEL", ``fe_sw2_bc_vel``), 1 for
   a weak depth boundary ("DEPTH", ``fe_sw2_bc_h``), 2 for a discharge string
   (``fe_sw2_bc_discharge``, src/models/sw2/sw2_bc_discharge.c.bk) and 3 for a
-  tailwater string (``fe_sw2_bc_tailwater``, sw2_bc_tailwater.c.bk);
+  tailwater string (``fe_sw2_bc_tailwater``, sw2_bc_tailwater.c.bk), 4 for an outflow
+  string (``fe_sw2_bc_outflow``) and 5 for a flux string (``fe_sw2_bc_flux``);
 * the node-major state ``[h, u, v]`` per node (dof = 3*node + var,
   src/structs/sivar_position/sivar_position.c:61-81);
 * time series: id 0 = boundary depth (hard-coded in src/models/sw2/sw2_bc_h.c:156),
   ids 1/2 = boundary velocity x/y, id 3 = the discharge string's series value,
-  id 4 = the tailwater elevation; ``bc_conveyance`` and ``bc_rough_height`` are the
+  id 4 = the tailwater elevation, id 5 = the flux strings' unit flux (inflow positive); ``bc_conveyance`` and ``bc_rough_height`` are the
   discharge string's conveyance and the boundary strings' roughness height.
 
 The structured flume reproduces the node and triangle layout of the reference's
@@ -39,7 +40,7 @@ class SW2Case:
     xyz: np.ndarray          # (V,3) float64
     tri: np.ndarray          # (T,3) int32
     seg: np.ndarray          # (S,2) int32
-    seg_kind: np.ndarray     # (S,) int32: 0 velocity, 1 depth, 2 discharge, 3 tailwater
+    seg_kind: np.ndarray     # (S,) int32: 0 velocity, 1 depth, 2 discharge, 3 tailwater, 4 outflow, 5 flux
     sol0: np.ndarray         # (3V,) float64 initial [h,u,v] per node
     dt: float
     nsteps: int
@@ -51,7 +52,7 @@ class SW2Case:
     gravity: float = GRAVITY
     bc_conveyance: float = 1.0      # discharge string's conveyance (series 3 gives its series value)
     bc_rough_height: float = 0.0    # equivalent roughness height of the boundary strings
-    # series ids: 0 depth, 1/2 velocity x/y, 3 discharge series value, 4 tailwater elevation
+    # series ids: 0 depth, 1/2 velocity x/y, 3 discharge series value, 4 tailwater elevation, 5 unit flux
 
     @property
     def nnodes(self) -> int:
@@ -207,6 +208,18 @@ def flume_structures_case(nsteps: int = 20, npx: int = 21, npy: int = 6, q_unit:
     series[4] = _const_series(0.0, tf, z_down + tail_depth)
     return dataclasses.replace(base, name="flume_structures", seg_kind=kind, series=series,
                                bc_conveyance=conveyance, bc_rough_height=rough_height)
+
+
+def flume_flux_outflow_case(nsteps: int = 20, npx: int = 21, npy: int = 6, q_unit: float = 0.5) -> SW2Case:
+    """The flume of ``flume_case`` with a flux string on the x = 0 edge
+    (sw2_bc_flux.c.bk: the series value ``q_unit`` m^2/s carried in as an explicit
+    flux) and an outflow string on the x = 1000 edge (sw2_bc_outflow.c.bk: implicit
+    flow with the computed depth and velocity)."""
+    base = flume_case(nsteps=nsteps, npx=npx, npy=npy)
+    kind = np.where(base.seg_kind == 0, 5, 4).astype(np.int32)
+    series = dict(base.series)
+    series[5] = _const_series(0.0, base.dt * nsteps, float(q_unit))
+    return dataclasses.replace(base, name="flume_flux_outflow", seg_kind=kind, series=series)
 
 
 def still_beach_case(nsteps: int = 1440, npx: int = 16, npy: int = 6, nt: int = 1440) -> SW2Case:

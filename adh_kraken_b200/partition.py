@@ -479,6 +479,8 @@ class DeviceRankModel:
             qs = series_step_average(*s[3], t1, t2) if 3 in s else 0.0
             tw = series_step_average(*s[4], t1, t2) if 4 in s else 0.0
             self.model.set_bc_structures(qs, self.case.bc_conveyance, self.case.bc_rough_height, tw)
+        if 5 in s:
+            self.model.set_bc_flux(series_step_average(*s[5], t1, t2))
 
     def wd_flags(self, sol, sol_old):
         self._wd = self.model.wd_flags(sol, sol_old)

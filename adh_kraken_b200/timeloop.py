@@ -101,6 +101,8 @@ class SW2Simulation:
             qs = series_step_average(*s[3], t_new - dt, t_new) if 3 in s else 0.0
             tw = series_step_average(*s[4], t_new - dt, t_new) if 4 in s else 0.0
             self.model.set_bc_structures(qs, self.case.bc_conveyance, self.case.bc_rough_height, tw)
+        if 5 in s:              # flux segments
+            self.model.set_bc_flux(series_step_average(*s[5], t_new - dt, t_new))
         return t_new
 
     def _attempt(self, opts, dt):

@@ -40,7 +40,9 @@ typedef struct {
     const int *seg;         /* [2*nseg] boundary segments; node order gives the outward normal */
     const int *seg_kind;    /* [nseg] 0 = "NB VEL" (fe_sw2_bc_vel), 1 = "DEPTH" (fe_sw2_bc_h),
                                2 = discharge (fe_sw2_bc_discharge, src/models/sw2/sw2_bc_discharge.c.bk:57),
-                               3 = tailwater (fe_sw2_bc_tailwater, src/models/sw2/sw2_bc_tailwater.c.bk:57) */
+                               3 = tailwater (fe_sw2_bc_tailwater, src/models/sw2/sw2_bc_tailwater.c.bk:57),
+                               4 = outflow (fe_sw2_bc_outflow, src/models/sw2/sw2_bc_outflow.c.bk:58),
+                               5 = flux (fe_sw2_bc_flux, src/models/sw2/sw2_bc_flux.c.bk:58) */
     const int *indptr;      /* optional [3*nnodes+1]: the caller's CSR, checked against ours; NULL to build */
     const int *cols;        /* optional [nnz] */
     double gravity;         /* sm->gravity, 9.8 by default */
@@ -144,6 +146,10 @@ int sw2g_set_step(sw2g_model *m, double dt, double tau_temporal, double bc_depth
  * divides by zero (the residual turns non-finite).  Defaults: 0, 1, 0, 0.  Non-finite
  * values or a zero conveyance give SW2G_ERR_ARG. */
 int sw2g_set_bc_structures(sw2g_model *m, double q_series, double conveyance, double rough_height, double tail_elev);
+/* The series value of the flux strings (kind 5) for the coming steps: the unit flux
+ * whose negative the strings carry into the domain (sw2_bc_flux.c.bk:151-153).
+ * Default 0; a non-finite value gives SW2G_ERR_ARG. */
+int sw2g_set_bc_flux(sw2g_model *m, double flux_series);
 
 /* --- drop-in host-buffer entry points ------------------------------------ */
 /* fe_sw2_wdflag_legacy (src/models/sw2/sw2_wdflag_legacy.c:34): [ntri] flags 0/1/2 */

@@ -28,6 +28,7 @@ class _Model(C.Structure):
         ("bc_depth", C.c_double), ("bc_vx", C.c_double), ("bc_vy", C.c_double),
         ("wd_flag", _ip),
         ("bc_qs", C.c_double), ("bc_convey", C.c_double), ("bc_rough", C.c_double), ("bc_tail", C.c_double),
+        ("bc_flux", C.c_double),
     ]
 
 
@@ -131,6 +132,7 @@ class OracleModel:
         s = self.case.series
         self.m.bc_qs = series_average(*s[3], t1, t2) if 3 in s else 0.0
         self.m.bc_tail = series_average(*s[4], t1, t2) if 4 in s else 0.0
+        self.m.bc_flux = series_average(*s[5], t1, t2) if 5 in s else 0.0
 
     # -- kernels
     def wd_flags(self, sol, sol_old):

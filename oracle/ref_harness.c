@@ -507,10 +507,12 @@ static void mode_rect(int argc, char **argv) {
     out_rec("grad_shp", 'd', grad, 6 * (int64_t)g.nelems2d);
 }
 
-/* Mode "bcx": the discharge and tailwater segment residuals of sw2_bc_discharge.c.bk and
- * sw2_bc_tailwater.c.bk.  Those files are not part of the reference's build and do not
- * compile against its live structures (the discharge file reads a NULL str_values, the
- * tailwater file an older dof-map API), so their top-level steps are followed here line
+/* Mode "bcx": the discharge, tailwater, outflow and flux segment residuals of
+ * sw2_bc_discharge.c.bk, sw2_bc_tailwater.c.bk, sw2_bc_outflow.c.bk and sw2_bc_flux.c.bk
+ * (kinds 2-5; a flux record carries its series value in the q_series slot).  Those
+ * files are not part of the reference's build and do not compile against its live
+ * structures (the discharge file reads a NULL str_values, the others call an older
+ * dof-map API), so their top-level steps are followed here line
  * by line while every integral, the roughness law and the drag coefficient are the
  * reference's own compiled functions (fe_sw2_1d_explicit_flow, fe_sw2_1d_wall_friction,
  * fe_sw2_1d_implicit_flow, fe_sw2_1d_pressure in src/fe/fe_sw2_boundary_integrals.c,
@@ -559,6 +561,13 @@ static void bcx_one(const double *in, double *out) {
         double elem_avg_discharge = one_2 * (discharge[0] + discharge[1]);
         fe_sw2_1d_explicit_flow(out, elem1d, 0, nrml, djac, dt, elem_avg_discharge, h_avg, u, v, OFF, OFF);
         fe_sw2_1d_wall_friction(out, elem1d, 0, nrml, djac, dt, u, v, resistance, OFF, OFF);
+    } else if (kind == 4) {                /* sw2_bc_outflow.c.bk:144 */
+        fe_sw2_1d_implicit_flow(out, elem1d, 0, nrml, djac, dt, elem_vel, elem_head, OFF, OFF);
+    } else if (kind == 5) {                /* sw2_bc_flux.c.bk:114-116,151-153; the series value in the q_series slot */
+        double u[2] = {elem_vel[0].x, elem_vel[1].x}, v[2] = {elem_vel[0].y, elem_vel[1].y};
+        double h_avg = one_2 * (elem_head[0] + elem_head[1]); if (h_avg < SMALL) h_avg = SMALL;
+        double flux = -1.0 * qs;
+        fe_sw2_1d_explicit_flow(out, elem1d, 0, nrml, djac, dt, flux, h_avg, u, v, OFF, OFF);
     } else if (kind == 3) {                /* sw2_bc_tailwater.c.bk:152-170 */
         double elem_depth[2];
         elem_depth[0] = tail - z0;

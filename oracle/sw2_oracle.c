@@ -621,7 +621,8 @@ static void discharge_resid(const sw2o_model *m, v2 n, double djac, double dt, c
     wall_friction(elem_rhs, n, djac, dt, u, v, res);
 }
 /* fe_sw2_bc_vel (src/models/sw2/sw2_bc_vel.c:58), fe_sw2_bc_h (sw2_bc_h.c:57), and the
- * discharge and tailwater conditions of sw2_bc_discharge.c.bk / sw2_bc_tailwater.c.bk */
+ * discharge, tailwater, outflow and flux conditions of sw2_bc_discharge.c.bk,
+ * sw2_bc_tailwater.c.bk, sw2_bc_outflow.c.bk and sw2_bc_flux.c.bk */
 static void seg_resid(const sw2o_model *m, const double *sol, int k, double pert, int pnode, int pvar, int psign,
                       double *elem_rhs) {
     const int *nd = m->seg + 2 * k;
@@ -646,6 +647,13 @@ static void seg_resid(const sw2o_model *m, const double *sol, int k, double pert
         }
     } else if (m->seg_kind[k] == 2) {
         discharge_resid(m, n, djac, dt, head, vel, elem_rhs);
+    } else if (m->seg_kind[k] == 4) {   /* sw2_bc_outflow.c.bk:144 */
+        implicit_flow(elem_rhs, n, djac, dt, vel, head);
+    } else if (m->seg_kind[k] == 5) {   /* sw2_bc_flux.c.bk:151-153 */
+        double u[2] = {vel[0].x, vel[1].x}, v[2] = {vel[0].y, vel[1].y};
+        double h_avg = one_2 * (head[0] + head[1]);
+        if (h_avg < SMALL) h_avg = SMALL;
+        explicit_flow(elem_rhs, n, djac, dt, -1.0 * m->bc_flux, h_avg, u, v);
     } else {   /* sw2_bc_tailwater.c.bk:152-170: depth below the elevation at the first node, at both */
         double z0 = m->xyz[3 * nd[0] + 2];
         double dep[2] = {m->bc_tail - z0, m->bc_tail - z0};

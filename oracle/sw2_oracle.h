@@ -23,7 +23,8 @@ typedef struct {
     const int *tri;          /* 3*ntri, counter-clockwise */
     const int *seg;          /* 2*nseg, node order gives the outward normal */
     const int *seg_kind;     /* nseg: 0 = NB VEL (fe_sw2_bc_vel), 1 = DEPTH (fe_sw2_bc_h),
-                                2 = discharge (sw2_bc_discharge.c.bk), 3 = tailwater (sw2_bc_tailwater.c.bk) */
+                                2 = discharge (sw2_bc_discharge.c.bk), 3 = tailwater (sw2_bc_tailwater.c.bk),
+                                4 = outflow (sw2_bc_outflow.c.bk), 5 = flux (sw2_bc_flux.c.bk) */
     const double *tri_djac;  /* ntri: element area */
     const double *tri_grad;  /* 6*ntri: grad phi_a (x,y) for a = 0..2 */
     const double *seg_djac;  /* nseg: segment length */
@@ -40,6 +41,7 @@ typedef struct {
     double bc_convey;        /* discharge string's conveyance */
     double bc_rough;         /* boundary strings' equivalent roughness height */
     double bc_tail;          /* tailwater elevation */
+    double bc_flux;          /* flux string's series value */
 } sw2o_model;
 
 /* geometry: selem2d_get_triangle_linear_djac_nrml_gradPhi (src/structs/selem/selem_2d.c:270-350),
