@@ -69,7 +69,7 @@ def parse():
                    help="Newton test max|R| <= tol_rel * max|R(previous step)|; 0: the reference's absolute 1e-8")
     p.add_argument("--basis", type=int, choices=[32, 64], default=32,
                    help="fast path: FP32 (default) or FP64 GMRES basis around the FP32 preconditioner")
-    p.add_argument("--restart", type=int, default=50, help="GMRES restart length of both paths (1..200)")
+    p.add_argument("--restart", type=int, default=100, help="GMRES restart length of both paths (1..200)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
