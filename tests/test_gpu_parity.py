@@ -195,7 +195,7 @@ def test_undo_step_retries_the_interval():
 
 
 BENCH_OPTS = dict(tol_nonlin=1e-8, tol_nonlin_rel=1e-8, inc_nonlin=1e-6, max_nonlin_it=10, krylov_max_it=20000,
-                  krylov_tol=1e-6, precond=2, krylov_method=1, krylov_restart=50)
+                  krylov_tol=1e-6, precond=2, krylov_method=1, krylov_restart=100)
 
 
 @pytest.mark.parametrize("mode", ["reference_test", "bench_fast", "bench_plain"])
