@@ -188,6 +188,8 @@ class SW2Simulation:
         held = self.keep_reduced_dt > 0 and self.dt_hold is not None and self.dt_hold < self.case.dt
         if held:
             dt = self.dt_hold
+        h_start = dt
+        if held:
             if rel > 0:
                 # R(sol_old) scales with the step's length (sol = sol_old makes the temporal
                 # terms vanish), so rel x dt/h keeps the tolerance of the whole interval
@@ -227,7 +229,7 @@ class SW2Simulation:
                     grown = dt / DT_REDUCE_FACTOR
                     self.dt_hold = None if grown >= self.case.dt * (1 - NOT_QUITE_SMALL) else grown
                     self.hold_count = 0
-        out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts, "step_start": dt if held else self.case.dt,
+        out = {"success": int(ok), "substeps": len(subs), "dt_cuts": cuts, "step_start": h_start,
                "newton_its": sum(s["newton_its"] for s in subs + failed),
                "krylov_its": sum(s["krylov_its"] for s in subs + failed),
                "linear_unconverged": sum(s.get("linear_unconverged", 0) for s in subs + failed)}

@@ -123,3 +123,16 @@ def test_held_step_keeps_the_interval_tolerance():
     assert seen[0] == (q, pytest.approx(1e-8 / DT_REDUCE_FACTOR), 0.0)
     first_tol = 1e-8 * DT_REDUCE_FACTOR * (1e-8 / DT_REDUCE_FACTOR) / 1e-8 * 3.0
     assert all(s[1] == pytest.approx(1e-8) and s[2] == pytest.approx(first_tol) for s in seen[1:])
+
+
+def test_advance_reports_the_step_it_started_with():
+    case = flume_case(nsteps=8, npx=5, npy=3)
+    q = case.dt * DT_REDUCE_FACTOR
+    sim = SW2Simulation(case, model=FakeModel(dt_ok=q))
+    starts = [sim.advance()["step_start"] for _ in range(3)]
+    assert starts == [case.dt, q, q]
+    sim2 = SW2Simulation(case, model=FakeModel(dt_ok=q * DT_REDUCE_FACTOR))
+    sim2.advance()                       # two cuts: holds q / 4
+    sim2.model.dt_ok = q * DT_REDUCE_FACTOR ** 3
+    st = sim2.advance()                  # starts at q / 4, cuts twice more
+    assert st["step_start"] == q * DT_REDUCE_FACTOR and st["dt_cuts"] == 2
