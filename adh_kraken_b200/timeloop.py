@@ -77,6 +77,7 @@ class SW2Simulation:
         # step (the reference keeps a cut dt too: tc_scale writes sm->ts->dt and nothing
         # restores it); after keep_reduced_dt such intervals the step grows by 1/DT_REDUCE_FACTOR
         # toward the case's dt.  0 turns the carry-over off.
+        self._has_discharge = bool(np.any(np.asarray(case.seg_kind) == 2))
         self.keep_reduced_dt = 4
         self.dt_hold = None      # the reduced step carried over, None = the case's dt
         self.hold_count = 0      # intervals completed at dt_hold
@@ -97,6 +98,9 @@ class SW2Simulation:
         d, vx, vy = self.bc_values(t_new - dt, t_new)
         self.model.set_step(dt, d, vx, vy)
         s = self.case.series
+        if self._has_discharge and not self.case.bc_rough_height > np.finfo(np.float64).eps:
+            # the discharge law divides by the strings' drag, zero without a roughness height
+            raise ValueError("discharge segments need SW2Case.bc_rough_height > 0")
         if 3 in s or 4 in s:    # discharge / tailwater segments
             qs = series_step_average(*s[3], t_new - dt, t_new) if 3 in s else 0.0
             tw = series_step_average(*s[4], t_new - dt, t_new) if 4 in s else 0.0

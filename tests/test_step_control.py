@@ -136,3 +136,14 @@ def test_advance_reports_the_step_it_started_with():
     sim2.model.dt_ok = q * DT_REDUCE_FACTOR ** 3
     st = sim2.advance()                  # starts at q / 4, cuts twice more
     assert st["step_start"] == q * DT_REDUCE_FACTOR and st["dt_cuts"] == 2
+
+
+def test_discharge_segments_without_roughness_are_refused():
+    """The discharge law divides by the boundary strings' drag: a case with discharge
+    segments and no roughness height is refused before any step."""
+    import dataclasses
+    from adh_kraken_b200.mesh import flume_structures_case
+    case = dataclasses.replace(flume_structures_case(nsteps=2), bc_rough_height=0.0)
+    sim = SW2Simulation(case, model=FakeModel(dt_ok=case.dt))
+    with pytest.raises(ValueError):
+        sim.step()
