@@ -16,6 +16,15 @@ Readers follow the reference's own readers card for card:
   (d = 1, dof 3 node) or ``DA_VELOCITY`` (d = 2, dofs 3 node + 1, + 2), the names of
   the SW2 variables in sadh_def.c:28-33.
 
+* ``.params`` time series -- the series pass of smodel_super_read
+  (src/structs/smodel_super/smodel_super_read.c:42-61) with sseries_read_allocate
+  (src/structs/sseries/sseries.c:46-118): ``SERIES BC id n in_units out_units`` then n
+  lines ``t value``; the series gets id - 1, times are scaled by the input unit
+  (sdt_get_conversion_factor, src/structs/sdt/sdt.c:50: seconds, minutes, hours, days,
+  weeks; units outside 0..4 stop the reference, sdt_check_units :109).  ``SERIES WIND``
+  and ``SERIES WAVE`` (two station coordinates, then 2 or 3 values per line) are read past,
+  as the reference reads them into lists the SW2 step does not use.
+
 The reference splits ``.geo`` lines on single spaces and copies each into a
 100-byte buffer (sgrid_read.c:28); the writer uses single spaces, and its longest
 line (an ND card with a 10-digit id and three 24-character ``%.17g`` values) is 88
@@ -183,11 +192,60 @@ def write_init(path: str, sol, sol_old, sol_older, nelems: int = 0, t: float = 0
                 f.write("ENDDS\n")
 
 
+_UNIT_SECONDS = {0: 1, 1: 60, 2: 3600, 3: 86400, 4: 604800}   # sdt_get_conversion_factor (an int)
+
+
+def _tokens(line: str):
+    # get_token / get_next_token (src/tokens/tokens.c:10-40): strtok on " \t\n"
+    return line.replace("\t", " ").replace("\n", " ").split(" ")
+
+
+def read_params_series(path: str) -> Dict[int, tuple]:
+    """The ``SERIES BC`` time series of a ``.params`` file as the reference reads them:
+    {id (file id - 1): (times in seconds, values)}, in file order."""
+    out: Dict[int, tuple] = {}
+    with open(path) as fh:
+        lines = fh.readlines()
+    i = 0
+    while i < len(lines):
+        tok = [t for t in _tokens(lines[i]) if t]
+        i += 1
+        if not tok or tok[0] != "SERIES" or len(tok) < 2:
+            continue
+        kind = tok[1]
+        if kind not in ("BC", "WIND", "WAVE"):
+            raise ValueError(f"{path}:{i}: series type {kind} not recognised")
+        rest = tok[2:]
+        sid, n = int(rest[0]) - 1, int(rest[1])
+        if kind in ("WIND", "WAVE"):
+            rest = rest[2:]             # station x, y
+        in_units, out_units = int(rest[2]), int(rest[3])
+        for u, what in ((in_units, "input"), (out_units, "output")):
+            if u not in _UNIT_SECONDS:
+                raise ValueError(f"{path}:{i}: invalid {what} time units {u} (0..4)")
+        nval = {"BC": 1, "WIND": 2, "WAVE": 3}[kind]
+        times = np.empty(n)
+        values = np.empty((n, nval))
+        for k in range(n):
+            et = [t for t in _tokens(lines[i]) if t]
+            i += 1
+            times[k] = float(et[0]) * _UNIT_SECONDS[in_units]
+            for v in range(nval):
+                values[k, v] = float(et[1 + v]) if 1 + v < len(et) else -999.0
+        if kind == "BC":
+            out[sid] = (times, values[:, 0].copy())
+    return out
+
+
 def case_from_files(name: str, geo_path: str, init_path: str, seg_kind, dt: float, nsteps: int,
                     series, t0: float = 0.0, **kw) -> SW2Case:
     """An SW2Case from a ``.geo`` grid and an ``.init`` state.  ``seg_kind`` gives each
-    segment's boundary (0 NB VEL, 1 DEPTH): an array over the segments, or a dict from
-    the SEG cards' bflag to the kind.  The case starts from the file's current level."""
+    segment's boundary (0 NB VEL, 1 DEPTH, 2-5 the structure strings): an array over the
+    segments, or a dict from the SEG cards' bflag to the kind.  ``series`` is a dict of
+    time series or the path of a ``.params`` file to read them from.  The case starts
+    from the file's current level."""
+    if isinstance(series, str):
+        series = read_params_series(series)
     g = read_geo(geo_path)
     if isinstance(seg_kind, dict):
         kinds = np.array([seg_kind[int(b)] for b in g.seg_bflag], dtype=np.int32)

@@ -599,6 +599,47 @@ static int mode_bcx(const char *in_path, const char *out_path) {
     return 0;
 }
 
+/* Mode "params": the series pass of smodel_super_read
+ * (src/structs/smodel_super/smodel_super_read.c:42-61) on a .params file, through the
+ * reference's own tokenizer and sseries_read_allocate; output records "ids", "sizes",
+ * "times" and "values" of the BC series in list order.  WIND and WAVE series are not
+ * handled here (their station arrays need a node count). */
+static int mode_params(const char *in_path, const char *out_path) {
+    FILE *fp = fopen(in_path, "r");
+    if (!fp) { fprintf(stderr, "harness: cannot read %s\n", in_path); return 2; }
+    SSERIES *head = NULL, *curr = NULL;
+    char *line = NULL, *token = NULL;
+    size_t len = 0;
+    while (getline(&line, &len, fp) != -1) {
+        get_token(line, &token); if (token == NULL) continue;
+        if (strcmp(token, "SERIES") == 0) {
+            get_next_token(&token);
+            if (token && strcmp(token, "BC") == 0)
+                sseries_read_allocate(fp, &head, &curr, TIME_SERIES, &token, UNSET_INT);
+            else { fprintf(stderr, "harness: series type not handled\n"); fclose(fp); return 2; }
+        }
+    }
+    fclose(fp);
+    int n = 0, tot = 0;
+    for (SSERIES *p = head; p; p = p->next) { n++; tot += p->size; }
+    int *ids = malloc(sizeof(int) * (n + 1)), *sizes = malloc(sizeof(int) * (n + 1));
+    double *times = malloc(sizeof(double) * (tot + 1)), *vals = malloc(sizeof(double) * (tot + 1));
+    int k = 0, e = 0;
+    for (SSERIES *p = head; p; p = p->next, k++) {
+        ids[k] = p->id; sizes[k] = p->size;
+        for (int j = 0; j < p->size; j++, e++) { times[e] = p->entry[j].time; vals[e] = p->entry[j].value[0]; }
+    }
+    g_out = fopen(out_path, "wb");
+    if (!g_out) { fprintf(stderr, "harness: cannot write %s\n", out_path); return 2; }
+    out_rec("ids", 'i', ids, n);
+    out_rec("sizes", 'i', sizes, n);
+    out_rec("times", 'd', times, tot);
+    out_rec("values", 'd', vals, tot);
+    fclose(g_out);
+    free(ids); free(sizes); free(times); free(vals);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc >= 4 && strcmp(argv[1], "geo") == 0) {
         if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
@@ -609,6 +650,12 @@ int main(int argc, char **argv) {
         mode_geo(argv);
         fclose(g_out);
         return 0;
+    }
+    if (argc >= 4 && strcmp(argv[1], "params") == 0) {
+        if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }
+        debug_initialize();
+        sadh_def_init();
+        return mode_params(argv[2], argv[3]);
     }
     if (argc >= 4 && strcmp(argv[1], "bcx") == 0) {
         if (getenv("HARNESS_VERBOSE") == NULL) { if (!freopen("/dev/null", "w", stdout)) return 2; }

@@ -126,3 +126,15 @@ def run_bcx(records):
             f.write(rec.tobytes())
         out = run_harness("bcx", in_path=p)
     return out["seg_resid"].reshape(-1, 6)
+
+
+def run_params_series(path):
+    """The BC time series of a ``.params`` file as the reference's own reader builds them
+    (harness mode ``params``): {id: (times, values)} in list order."""
+    out = run_harness("params", in_path=path)
+    ids, sizes = out["ids"], out["sizes"]
+    res, e = {}, 0
+    for sid, n in zip(ids.tolist(), sizes.tolist()):
+        res[int(sid)] = (out["times"][e:e + n], out["values"][e:e + n])
+        e += n
+    return res

@@ -1,6 +1,7 @@
-"""The .geo and .init readers and writers (adh_kraken_b200/deck.py) against the
-reference's own readers, sgrid_read and smodel_super_read_init, run through the
-compiled harness (oracle/_ref/); no GPU."""
+"""The .geo and .init readers and writers and the .params series reader
+(adh_kraken_b200/deck.py) against the reference's own readers, sgrid_read,
+smodel_super_read_init and sseries_read_allocate, run through the compiled harness
+(oracle/_ref/); no GPU."""
 import os
 
 import numpy as np
@@ -9,7 +10,9 @@ import pytest
 from adh_kraken_b200.deck import case_from_files, read_geo, read_init, write_geo, write_init
 from adh_kraken_b200.mesh import flume_case, small_delaunay_case
 from oracle.oracle import OracleModel
+from oracle import refio
 from oracle.refio import harness_available, run_harness
+from adh_kraken_b200 import deck
 
 needs_harness = pytest.mark.skipif(not harness_available(), reason="reference harness not built")
 from fixtures import reference_src
@@ -151,3 +154,52 @@ def test_case_from_files_steps_like_the_original(tmp_path):
     a, ha = OracleModel(case).run(2)
     b, hb = OracleModel(c2).run(2)
     assert np.array_equal(a, b) and [h["newton_its"] for h in ha] == [h["newton_its"] for h in hb]
+
+
+PARAMS_TEXT = """MODEL 1 SW2
+# series in several time units, with tabs and blank lines
+SERIES BC 1 3 0 0
+0 2.0
+3600\t2.5
+7200 2.25
+
+SERIES BC 3 4 2 0
+0   0.1
+0.5 0.2
+1.25 0.35
+2 0.1e-1
+IP NTL 1e-6
+SERIES BC 2 2 1 1
+0 -0.125
+90 3.3333333333333335
+BC 3 SW2 NB VEL 1
+"""
+
+
+@pytest.mark.skipif(not refio.harness_available(), reason="reference harness not built")
+def test_params_series_match_the_reference_reader(tmp_path):
+    """The .params series pass reads what the reference's sseries_read_allocate reads,
+    bit for bit: ids, times scaled by the input unit, values."""
+    p = tmp_path / "deck.params"
+    p.write_text(PARAMS_TEXT)
+    files = [str(p)]
+    src = reference_src()
+    if src is not None:
+        files += [os.path.join(os.path.dirname(src), "qa", "flume", f) for f in ("test_sm1.params", "test_sm2.params")]
+    for f in files:
+        ours = deck.read_params_series(f)
+        ref = refio.run_params_series(f)
+        assert list(ours) == list(ref), f
+        for k in ours:
+            assert np.array_equal(ours[k][0], ref[k][0]) and np.array_equal(ours[k][1], ref[k][1]), (f, k)
+    ours = deck.read_params_series(str(p))
+    assert sorted(ours) == [0, 1, 2]
+    assert ours[2][0].tolist() == [0.0, 1800.0, 4500.0, 7200.0]      # hours
+    assert ours[1][0].tolist() == [0.0, 5400.0]                       # minutes
+
+
+def test_params_series_refuse_bad_units(tmp_path):
+    p = tmp_path / "bad.params"
+    p.write_text("SERIES BC 1 1 7 0\n0 1\n")
+    with pytest.raises(ValueError):
+        deck.read_params_series(str(p))
